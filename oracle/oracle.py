@@ -1,0 +1,267 @@
+"""ctypes front end of the C parity oracle (astro_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py as the checker / timed CPU baseline.  The
+astrofd_b200 product never imports this module.
+
+The functions mirror the reference's Python call surface
+(core/srhd_core.py, core/rmhd_core.py, core/boundary.py, core/nozzle.py,
+core/source_terms.py) on numpy float64 arrays.
+"""
+import ctypes as C
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+class OParams(C.Structure):
+    _fields_ = [("physics", C.c_int), ("recon", C.c_int), ("limiter", C.c_int),
+                ("riemann", C.c_int), ("n_passive", C.c_int),
+                ("passive_offset", C.c_int), ("resistive", C.c_int),
+                ("pad_", C.c_int), ("gamma", C.c_double), ("p_max", C.c_double),
+                ("v_max", C.c_double), ("glm_ch", C.c_double),
+                ("glm_cp", C.c_double), ("resistivity", C.c_double)]
+
+
+class ONozzle(C.Structure):
+    _fields_ = [("ng", C.c_int), ("profile", C.c_int), ("perturb", C.c_int),
+                ("physics", C.c_int), ("b_init", C.c_int), ("n_tracers", C.c_int),
+                ("tracer_offset", C.c_int), ("two_temperature", C.c_int),
+                ("thermo_offset", C.c_int), ("pad_", C.c_int),
+                ("radius", C.c_double), ("shear_thick", C.c_double),
+                ("gamma_jet", C.c_double), ("eta_rho", C.c_double),
+                ("p_eq", C.c_double), ("rho_amb", C.c_double),
+                ("vx_amb", C.c_double), ("vy_amb", C.c_double),
+                ("vz_amb", C.c_double), ("turb_vamp", C.c_double),
+                ("turb_pamp", C.c_double), ("b0", C.c_double), ("te", C.c_double),
+                ("ti", C.c_double), ("tracer_nozzle", C.c_double * 8),
+                ("tracer_amb", C.c_double * 8)]
+
+
+_lib = None
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        L.oracle_rhs.argtypes = [C.POINTER(OParams), dp, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, C.c_double, C.c_double, C.c_double, dp]
+        L.oracle_step.argtypes = [C.POINTER(OParams), dp, C.c_int, C.c_int, C.c_int,
+                                  C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_double, C.c_int, dp]
+        L.oracle_p2c.argtypes = [C.POINTER(OParams), dp, dp, C.c_long]
+        L.oracle_c2p.argtypes = [C.POINTER(OParams), dp, dp, C.c_long]
+        L.oracle_c2p_counters.argtypes = [C.POINTER(C.c_long), C.c_int]
+        L.oracle_max_char_speed.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.oracle_max_char_speed.restype = C.c_double
+        for f in (L.oracle_periodic_yz, L.oracle_outflow_right_x):
+            f.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.oracle_nozzle_left_x.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_double, C.c_double, C.c_int, C.c_int,
+                                           C.c_double, C.c_double,
+                                           C.POINTER(ONozzle), dp]
+        L.oracle_nozzle_left_x.restype = C.c_long
+        L.oracle_cooling.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_double, C.c_double, C.c_double, C.c_double]
+        L.oracle_two_temperature.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.c_int, C.c_double, C.c_double, C.c_int]
+        L.oracle_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+_RECON = {"muscl": 0, "ppm": 1, "weno": 2}
+_LIMITER = {"mc": 0, "minmod": 1, "vanleer": 2}
+
+
+def params_from_config(physics, cfg):
+    """Restates configure() (srhd_core.py:18-41, rmhd_core.py:21-50)."""
+    p = OParams()
+    p.physics = 0 if physics == "srhd" else 1
+    p.recon = _RECON.get(str(cfg.get("RECON", "muscl")).lower(), 0)
+    p.limiter = _LIMITER.get(str(cfg.get("LIMITER", "mc")).lower(), 0)
+    r = str(cfg.get("RIEMANN", "hlle")).lower()
+    if physics == "srhd":
+        p.riemann = 1 if r == "hllc" else 0
+    else:
+        p.riemann = 2 if r == "hlld_full" else (1 if r == "hlld" else 0)
+    p.n_passive = int(cfg.get("N_PASSIVE", 0))
+    p.passive_offset = int(cfg.get("PASSIVE_OFFSET", 5 if physics == "srhd" else 9))
+    p.resistive = 1 if cfg.get("RESISTIVE_ENABLED", False) else 0
+    p.gamma = float(cfg.get("GAMMA", 5.0 / 3.0))
+    p.p_max = float(cfg.get("P_MAX", 1.0))
+    p.v_max = float(cfg.get("V_MAX", 0.999))
+    p.glm_ch = float(cfg.get("GLM_CH", 1.0))
+    p.glm_cp = float(cfg.get("GLM_CP", 0.1))
+    p.resistivity = float(cfg.get("RESISTIVITY", 0.0))
+    return p
+
+
+def rhs(params, pr, dx, dy, dz):
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    nm = 5 if params.physics == 0 else 9
+    out = np.zeros((nm + params.n_passive,) + pr.shape[1:])
+    rc = lib().oracle_rhs(C.byref(params), _dp(pr), *pr.shape, dx, dy, dz, _dp(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rhs failed ({rc})")
+    return out
+
+
+def step(params, pr, dx, dy, dz, dt, rk):
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    out = np.zeros_like(pr)
+    rc = lib().oracle_step(C.byref(params), _dp(pr), *pr.shape, dx, dy, dz, dt, rk, _dp(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_step failed ({rc})")
+    return out
+
+
+def p2c(params, q):
+    q = np.ascontiguousarray(q, dtype=np.float64)
+    out = np.zeros_like(q)
+    lib().oracle_p2c(C.byref(params), _dp(q), _dp(out), q.shape[1])
+    return out
+
+
+def c2p(params, U):
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    out = np.zeros_like(U)
+    lib().oracle_c2p(C.byref(params), _dp(U), _dp(out), U.shape[1])
+    return out
+
+
+def c2p_counters(reset=True):
+    a = (C.c_long * 3)()
+    lib().oracle_c2p_counters(a, 1 if reset else 0)
+    return dict(newton=a[0], bisect=a[1], hydro_fallback=a[2])
+
+
+def max_char_speed(pr):
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    return lib().oracle_max_char_speed(_dp(pr), *pr.shape)
+
+
+def apply_periodic_yz(pr, ng):
+    assert pr.flags.c_contiguous and pr.dtype == np.float64
+    lib().oracle_periodic_yz(_dp(pr), *pr.shape, ng)
+
+
+def apply_outflow_right_x(pr, ng):
+    assert pr.flags.c_contiguous and pr.dtype == np.float64
+    lib().oracle_outflow_right_x(_dp(pr), *pr.shape, ng)
+
+
+_PROFILE = {"taper": 1, "smooth": 1, "parabolic": 2, "parabola": 2}
+
+
+def nozzle_struct(cfg):
+    c = ONozzle()
+    c.ng = int(cfg["NG"])
+    c.profile = _PROFILE.get(cfg.get("NOZZLE_PROFILE", "top_hat"), 0)
+    c.perturb = 0 if cfg.get("NOZZLE_PERTURB", "none") == "none" else 1
+    c.physics = 1 if cfg.get("PHYSICS") in ("rmhd", "grmhd") else 0
+    b = cfg.get("B_INIT")
+    c.b_init = 1 if b == "poloidal" else (2 if b == "toroidal" else 0)
+    c.n_tracers = int(cfg.get("N_TRACERS", 0))
+    c.tracer_offset = int(cfg.get("TRACER_OFFSET", 5))
+    c.two_temperature = 1 if cfg.get("TWO_TEMPERATURE", False) else 0
+    c.thermo_offset = int(cfg.get("THERMO_OFFSET", 0))
+    c.radius = cfg["JET_RADIUS"]
+    c.shear_thick = cfg["SHEAR_THICK"]
+    c.gamma_jet = cfg["GAMMA_JET"]
+    c.eta_rho = cfg["ETA_RHO"]
+    c.p_eq = cfg["P_EQ"]
+    c.rho_amb = cfg["RHO_AMB"]
+    c.vx_amb, c.vy_amb, c.vz_amb = cfg["VX_AMB"], cfg["VY_AMB"], cfg["VZ_AMB"]
+    c.turb_vamp = cfg.get("TURB_VAMP", 0.0)
+    c.turb_pamp = cfg.get("TURB_PAMP", 0.0)
+    c.b0 = cfg.get("B0", 0.0)
+    c.te = float(cfg.get("TE_NOZZLE", cfg.get("TE_AMB", 0.0)) or 0.0)
+    c.ti = float(cfg.get("TI_NOZZLE", cfg.get("TI_AMB", 0.0)) or 0.0)
+    nv = cfg.get("TRACER_NOZZLE_VALUES", []) or []
+    av = cfg.get("TRACER_AMB_VALUES", []) or []
+    for t in range(min(c.n_tracers, 8)):
+        c.tracer_nozzle[t] = nv[t] if t < len(nv) else (1.0 if t == 0 else 0.0)
+        c.tracer_amb[t] = av[t] if t < len(av) else 0.0
+    return c
+
+
+def nozzle_draw_count(cfg, dy, dz, ny_loc, nz_loc, y0, z0):
+    """Number of rng.random() draws apply_nozzle_left_x makes (nozzle.py:50-53)."""
+    if cfg.get("NOZZLE_PERTURB", "none") == "none":
+        return 0
+    from_weight = 0
+    ng = cfg["NG"]
+    prof = cfg.get("NOZZLE_PROFILE", "top_hat")
+    for j in range(ng, ng + ny_loc):
+        y = (j - ng + 0.5) * dy
+        for k in range(ng, ng + nz_loc):
+            z = (k - ng + 0.5) * dz
+            rr = math.sqrt((y - y0) ** 2 + (z - z0) ** 2)
+            if _weight(rr, cfg["JET_RADIUS"], cfg["SHEAR_THICK"], prof) > 0.0:
+                from_weight += 1
+    return 3 * ng * from_weight
+
+
+def _weight(r, radius, shear, profile):
+    if radius <= 0.0:
+        return 0.0
+    if profile in ("taper", "smooth"):
+        return 0.0 if r >= radius else 0.5 * (1.0 + math.cos(math.pi * r / radius))
+    if profile in ("parabolic", "parabola"):
+        if r >= radius:
+            return 0.0
+        x = r / radius
+        return max(0.0, 1.0 - x * x)
+    if shear > 0.0:
+        return 0.5 * (1.0 - math.tanh((r - radius) / shear))
+    return 1.0 if r <= radius else 0.0
+
+
+def apply_nozzle_left_x(pr, dx, dy, dz, ny_loc, nz_loc, y0, z0, rng, cfg):
+    assert pr.flags.c_contiguous and pr.dtype == np.float64
+    c = nozzle_struct(cfg)
+    n = nozzle_draw_count(cfg, dy, dz, ny_loc, nz_loc, y0, z0)
+    rnd = rng.random(n) if n > 0 else np.zeros(1)
+    used = lib().oracle_nozzle_left_x(_dp(pr), *pr.shape, dy, dz, ny_loc, nz_loc, y0, z0,
+                                      C.byref(c), _dp(rnd))
+    assert used == n, (used, n)
+
+
+def apply_cooling_heating(pr, dt, cfg):
+    if not cfg.get("COOLING_ENABLED", False):
+        return pr
+    lib().oracle_cooling(_dp(pr), *pr.shape, int(cfg.get("NG", 2)), dt,
+                         float(cfg.get("COOLING_LAMBDA", 0.0)),
+                         float(cfg.get("HEATING_RATE", 0.0)), float(cfg.get("P_MAX", 1.0)))
+    return pr
+
+
+def apply_two_temperature(pr, dt, cfg):
+    if not cfg.get("TWO_TEMPERATURE", False):
+        return pr
+    lib().oracle_two_temperature(_dp(pr), *pr.shape, int(cfg.get("NG", 2)), dt,
+                                 float(cfg.get("TEI_TAU", 0.5)),
+                                 int(cfg.get("THERMO_OFFSET", 0)))
+    return pr
+
+
+def num_threads():
+    return lib().oracle_num_threads()

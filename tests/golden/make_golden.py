@@ -1,0 +1,296 @@
+#!/usr/bin/env python3
+"""Generate the golden parity fixtures by running the reference itself.
+
+Test infrastructure only.  This script imports the reference's own Numba
+hot path (core/srhd_core.py, core/rmhd_core.py, core/boundary.py,
+core/nozzle.py, core/source_terms.py) read-only from a checkout of AstroFD
+and records its outputs on seeded inputs as ``.npz`` files next to this
+script.  The reference freezes its ``configure()`` globals at the first Numba
+compile (core/srhd_core.py:18, core/rmhd_core.py:21), so every configuration
+runs in a fresh subprocess.
+
+Usage:
+    python tests/golden/make_golden.py --ref <path-to-AstroFD> [--jobs 4] [names...]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+import numpy as np  # noqa: E402
+from cases import CASES, CASE_BY_NAME, DT_FRACTION  # noqa: E402
+import states  # noqa: E402
+
+SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
+           "c2p_rmhd", "c2p_srhd", "source_terms", "c1_run", "c5_run"]
+
+NOZZLE_BASE = dict(JET_RADIUS=0.1, SHEAR_THICK=0.02, NOZZLE_PROFILE="top_hat",
+                   GAMMA_JET=7.088812050083354, ETA_RHO=0.1, P_EQ=0.01,
+                   RHO_AMB=1.0, VX_AMB=0.0, VY_AMB=0.0, VZ_AMB=0.0,
+                   NOZZLE_PERTURB="none", TURB_VAMP=0.0, TURB_PAMP=0.0,
+                   N_TRACERS=0, TWO_TEMPERATURE=False, PHYSICS="hydro",
+                   B_INIT="none", B0=0.0)
+
+
+def _import_ref(ref):
+    sys.path.insert(0, ref)
+    from core import srhd_core, rmhd_core, boundary, nozzle, source_terms
+    return srhd_core, rmhd_core, boundary, nozzle, source_terms
+
+
+def run_case(name, ref, out):
+    S, R, B, N, ST = _import_ref(ref)
+    c = CASE_BY_NAME[name]
+    p = c["params"]
+    mod = S if c["physics"] == "srhd" else R
+    mod.configure(p)
+    pr = states.make_state(c["seed"], c["n"], c["ng"], c["physics"],
+                           c["n_extra"] + c["pad"], **c["state"])
+    n = pr.shape[1]
+    dx = dy = dz = 1.0 / c["n"]
+    if c["physics"] == "srhd":
+        rhs_fn = {"muscl": S.compute_rhs_muscl, "ppm": S.compute_rhs_ppm,
+                  "weno": S.compute_rhs_weno}[p["RECON"]]
+    else:
+        rhs_fn = {"muscl": R.compute_rhs_rmhd, "ppm": R.compute_rhs_ppm,
+                  "weno": R.compute_rhs_weno}[p["RECON"]]
+    rhs = rhs_fn(pr, n, n, n, dx, dy, dz)
+    dt = DT_FRACTION * dx
+    step = mod.step_ssprk3 if c["rk"] == 3 else mod.step_ssprk2
+    out_pr = step(pr.copy(), dx, dy, dz, dt)
+    extra = {}
+    if c["physics"] == "srhd":
+        extra["max_char_speed"] = np.array(S.max_char_speed(pr, n, n, n))
+    np.savez_compressed(out, pr_in=pr, rhs=rhs, step_out=out_pr,
+                        dt=np.array(dt), params=json.dumps(p), **extra)
+
+
+def _bc_setup(name):
+    """State plus nozzle config for the ghost-fill fixtures."""
+    cfg = dict(NOZZLE_BASE)
+    if name == "bc_srhd":
+        pr = states.make_state(301, 10, 2, "srhd")
+        cfg.update(NG=2, NOZZLE_PERTURB="random", TURB_VAMP=0.02, TURB_PAMP=0.01,
+                   SHEAR_THICK=0.02)
+        seed = 1234
+    elif name == "bc_srhd_tracers":
+        pr = states.make_state(302, 10, 3, "srhd", n_extra=3)
+        cfg.update(NG=3, N_TRACERS=1, TRACER_OFFSET=5, TRACER_NOZZLE_VALUES=[1.0],
+                   TRACER_AMB_VALUES=[0.0], TWO_TEMPERATURE=True, THERMO_OFFSET=6,
+                   TE_NOZZLE=0.5, TI_NOZZLE=0.25, SHEAR_THICK=0.0,
+                   NOZZLE_PROFILE="parabolic", NOZZLE_PERTURB="random",
+                   TURB_VAMP=0.05, TURB_PAMP=0.0)
+        seed = 77
+    elif name == "bc_rmhd_pol":
+        pr = states.make_state(303, 10, 3, "rmhd")
+        cfg.update(NG=3, PHYSICS="rmhd", B_INIT="poloidal", B0=0.05,
+                   NOZZLE_PROFILE="taper")
+        seed = 5
+    else:  # bc_rmhd_tor
+        pr = states.make_state(304, 10, 2, "rmhd", n_extra=2)
+        cfg.update(NG=2, PHYSICS="rmhd", B_INIT="toroidal", B0=0.3,
+                   TWO_TEMPERATURE=True, THERMO_OFFSET=9, TE_NOZZLE=0.02,
+                   TI_NOZZLE=0.03, NOZZLE_PERTURB="random", TURB_VAMP=0.01,
+                   TURB_PAMP=0.02, SHEAR_THICK=0.05)
+        seed = 9
+    return pr, cfg, seed
+
+
+def run_bc(name, ref, out):
+    S, R, B, N, ST = _import_ref(ref)
+    pr, cfg, seed = _bc_setup(name)
+    ng = cfg["NG"]
+    nint = pr.shape[2] - 2 * ng
+    d = 1.0 / nint
+    rng = np.random.default_rng(seed)
+    after = pr.copy()
+    B.apply_periodic_yz(after, ng)
+    periodic = after.copy()
+    B.apply_outflow_right_x(after, ng)
+    N.apply_nozzle_left_x(after, d, d, d, nint, nint, 0.5, 0.5, rng, cfg)
+    np.savez_compressed(out, pr_in=pr, periodic=periodic, filled=after,
+                        rng_seed=np.array(seed), cfg=json.dumps(cfg))
+
+
+def run_c2p(name, ref, out):
+    S, R, B, N, ST = _import_ref(ref)
+    if name == "c2p_rmhd":
+        R.configure(dict(GAMMA=4.0 / 3.0, P_MAX=1e3, V_MAX=0.9999))
+        pr = states.make_c2p_batch(401, 3000)
+        # also some states with B perpendicular to v (p2c/c2p consistent)
+        pr2 = states.make_c2p_batch(402, 1000)
+        v = pr2[1:4]
+        b = pr2[5:8]
+        b -= v * (np.sum(v * b, axis=0) / np.maximum(np.sum(v * v, axis=0), 1e-300))
+        pr = np.concatenate([pr, pr2], axis=1)
+        m = pr.shape[1]
+        U = np.zeros_like(pr)
+        out_pr = np.zeros_like(pr)
+        for c in range(m):
+            U[:, c] = R.prim_to_cons_rmhd(*pr[:, c], 4.0 / 3.0)
+        for c in range(m):
+            out_pr[:, c] = R.cons_to_prim_rmhd(*U[:, c])
+        np.savez_compressed(out, pr_in=pr, cons=U, pr_out=out_pr,
+                            params=json.dumps(dict(GAMMA=4.0 / 3.0, P_MAX=1e3,
+                                                   V_MAX=0.9999)))
+    else:
+        S.configure(dict(GAMMA=5.0 / 3.0, P_MAX=2.0, V_MAX=0.9999))
+        rng = np.random.default_rng(403)
+        m = 3000
+        pr = np.zeros((5, m))
+        pr[0] = 10.0 ** rng.uniform(-4, 1, m)
+        W = 10.0 ** rng.uniform(0, np.log10(20.0), m)
+        v = np.sqrt(1 - 1 / W ** 2)
+        d = rng.normal(size=(3, m))
+        d /= np.linalg.norm(d, axis=0)
+        pr[1:4] = v * d
+        pr[4] = 10.0 ** rng.uniform(-6, np.log10(2.0), m)
+        U = np.zeros_like(pr)
+        out_pr = np.zeros_like(pr)
+        for c in range(m):
+            U[:, c] = S.prim_to_cons(*pr[:, c])
+        for c in range(m):
+            out_pr[:, c] = S.cons_to_prim(*U[:, c])
+        np.savez_compressed(out, pr_in=pr, cons=U, pr_out=out_pr,
+                            params=json.dumps(dict(GAMMA=5.0 / 3.0, P_MAX=2.0,
+                                                   V_MAX=0.9999)))
+
+
+def run_source(name, ref, out):
+    S, R, B, N, ST = _import_ref(ref)
+    pr = states.make_state(501, 8, 3, "rmhd", n_extra=2)
+    pr[9] = np.abs(pr[9]) * 0.02
+    pr[10] = np.abs(pr[10]) * 0.03
+    cfg = dict(COOLING_ENABLED=True, COOLING_LAMBDA=0.01, HEATING_RATE=1e-4,
+               NG=3, P_MAX=2.0, TWO_TEMPERATURE=True, TEI_TAU=0.1,
+               THERMO_OFFSET=9, N_TRACERS=0)
+    dt = 0.01
+    a = pr.copy()
+    ST.apply_cooling_heating(a, dt, cfg)
+    b = a.copy()
+    ST.apply_two_temperature(b, dt, cfg)
+    np.savez_compressed(out, pr_in=pr, cooled=a, two_temp=b, dt=np.array(dt),
+                        cfg=json.dumps(cfg))
+
+
+def _run_loop(ref, physics, n, ng, params, cfg, steps, seed, sources=None):
+    """Reference driver loop (solvers/srhd3d_mpi_muscl.py:276-326) on one rank."""
+    S, R, B, N, ST = _import_ref(ref)
+    mod = S if physics == "srhd" else R
+    mod.configure(params)
+    rng = np.random.default_rng(seed)
+    Nn = n + 2 * ng
+    nm = 5 if physics == "srhd" else 9
+    nv = nm + params.get("N_PASSIVE", 0)
+    pr = np.zeros((nv, Nn, Nn, Nn))
+    pr[0] = 1.0 * (1.0 + 0.01 * (2.0 * rng.random((Nn, Nn, Nn)) - 1.0))
+    pr[4] = 0.01
+    if physics == "rmhd":
+        pr[5] = cfg.get("BX_AMB", 0.0)
+        pr[1:4] += 0.01 * (2.0 * rng.random((3, Nn, Nn, Nn)) - 1.0)
+    if params.get("N_PASSIVE", 0) == 2:
+        pr[nm] = 0.01
+        pr[nm + 1] = 0.01
+    pr0 = pr.copy()
+    d = 1.0 / n
+    brng = np.random.default_rng(1234)
+    B.apply_periodic_yz(pr, ng)
+    B.apply_outflow_right_x(pr, ng)
+    N.apply_nozzle_left_x(pr, d, d, d, n, n, 0.5, 0.5, brng, cfg)
+    dts = []
+    for _ in range(steps):
+        if physics == "srhd":
+            amax = S.max_char_speed(pr, Nn, Nn, Nn)
+        else:
+            amax = 1.0
+        dt = params["CFL"] * d / max(amax, 1e-12)
+        dts.append(dt)
+        B.apply_periodic_yz(pr, ng)
+        B.apply_outflow_right_x(pr, ng)
+        N.apply_nozzle_left_x(pr, d, d, d, n, n, 0.5, 0.5, brng, cfg)
+        step = mod.step_ssprk3 if params["RK_ORDER"] == 3 else mod.step_ssprk2
+        pr = step(pr, d, d, d, dt)
+        B.apply_periodic_yz(pr, ng)
+        B.apply_outflow_right_x(pr, ng)
+        N.apply_nozzle_left_x(pr, d, d, d, n, n, 0.5, 0.5, brng, cfg)
+        if sources is not None:
+            pr = ST.apply_cooling_heating(pr, dt, sources)
+            pr = ST.apply_two_temperature(pr, dt, sources)
+    return pr0, pr, np.array(dts)
+
+
+def run_loop(name, ref, out):
+    if name == "c1_run":
+        params = dict(GAMMA=5.0 / 3.0, P_MAX=2.0, V_MAX=0.9999, RECON="muscl",
+                      LIMITER="minmod", RIEMANN="hlle", RK_ORDER=2, CFL=0.4,
+                      N_PASSIVE=0, PASSIVE_OFFSET=5)
+        cfg = dict(NOZZLE_BASE, NG=2, SHEAR_THICK=0.0)
+        pr0, pr, dts = _run_loop(ref, "srhd", 16, 2, params, cfg, 10, 601)
+        np.savez_compressed(out, pr_init=pr0, pr_final=pr, dts=dts,
+                            params=json.dumps(params), cfg=json.dumps(cfg),
+                            steps=np.array(10), n=np.array(16), ng=np.array(2))
+    else:  # c5_run: magnetised WENO/HLLD jet with thermo passives + sources
+        params = dict(GAMMA=4.0 / 3.0, P_MAX=2.0, V_MAX=0.9999, RECON="weno",
+                      LIMITER="mc", RIEMANN="hlld_full", RK_ORDER=3, CFL=0.35,
+                      GLM_CH=1.0, GLM_CP=0.1, N_PASSIVE=2, PASSIVE_OFFSET=9,
+                      RESISTIVE_ENABLED=True, RESISTIVITY=1e-4)
+        cfg = dict(NOZZLE_BASE, NG=3, PHYSICS="rmhd", B_INIT="toroidal", B0=0.2,
+                   GAMMA_JET=10.0, TWO_TEMPERATURE=True, THERMO_OFFSET=9,
+                   TE_NOZZLE=0.1, TI_NOZZLE=0.1, BX_AMB=0.1)
+        sources = dict(COOLING_ENABLED=True, COOLING_LAMBDA=0.01, HEATING_RATE=0.0,
+                       NG=3, P_MAX=2.0, TWO_TEMPERATURE=True, TEI_TAU=0.1,
+                       THERMO_OFFSET=9, N_TRACERS=0)
+        pr0, pr, dts = _run_loop(ref, "rmhd", 10, 3, params, cfg, 3, 602, sources)
+        np.savez_compressed(out, pr_init=pr0, pr_final=pr, dts=dts,
+                            params=json.dumps(params), cfg=json.dumps(cfg),
+                            sources=json.dumps(sources), steps=np.array(3),
+                            n=np.array(10), ng=np.array(3))
+
+
+def one(name, ref):
+    out = os.path.join(HERE, name + ".npz")
+    if name in CASE_BY_NAME:
+        run_case(name, ref, out)
+    elif name.startswith("bc_"):
+        run_bc(name, ref, out)
+    elif name.startswith("c2p_"):
+        run_c2p(name, ref, out)
+    elif name == "source_terms":
+        run_source(name, ref, out)
+    else:
+        run_loop(name, ref, out)
+    print("wrote", out, flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", required=True)
+    ap.add_argument("--jobs", type=int, default=4)
+    ap.add_argument("--one", default=None)
+    ap.add_argument("names", nargs="*")
+    a = ap.parse_args()
+    if a.one:
+        one(a.one, a.ref)
+        return
+    names = a.names or ([c["name"] for c in CASES] + SPECIAL)
+    env = dict(os.environ, PYTHONDONTWRITEBYTECODE="1", NUMBA_NUM_THREADS="1")
+
+    def launch(nm):
+        r = subprocess.run([sys.executable, __file__, "--ref", a.ref, "--one", nm],
+                           env=env, capture_output=True, text=True)
+        if r.returncode != 0:
+            return f"FAIL {nm}\n{r.stdout}\n{r.stderr}"
+        return r.stdout.strip()
+
+    with ThreadPoolExecutor(a.jobs) as ex:
+        for msg in ex.map(launch, names):
+            print(msg, flush=True)
+
+
+if __name__ == "__main__":
+    main()
