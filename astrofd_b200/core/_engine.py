@@ -1,0 +1,168 @@
+"""Shared implementation behind the drop-in srhd_core / rmhd_core modules.
+
+``Engine`` holds the configured parameters of one physics module (the
+reference keeps them as Numba-frozen module globals, core/srhd_core.py:18-41,
+core/rmhd_core.py:21-50; here they are a POD struct passed by value to every
+kernel, so re-configuring takes effect immediately) and forwards array calls
+to libastrofd_b200.so.
+"""
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _lib, runtime as rt
+
+
+class Engine:
+    def __init__(self, physics):
+        self.physics = physics
+        self.nm = 5 if physics == _lib.SRHD else 9
+        self.p = _lib.AstroParams()
+        self.p.physics = physics
+        self.p.gamma = 5.0 / 3.0
+        self.p.srhd_gamma = 5.0 / 3.0
+        self.p.p_max = 1.0
+        self.p.v_max = 0.999
+        self.p.glm_ch = 1.0
+        self.p.glm_cp = 0.1
+        self.p.passive_offset = 5 if physics == _lib.SRHD else 9
+        self.p.flux_mode = _lib.FLUX_REFERENCE
+        self.p.precision = _lib.PREC_FP64
+        self.p.c2p_guess = _lib.GUESS_REFERENCE
+        self.stats = None
+
+    # -- configure() ------------------------------------------------------
+    def configure(self, params):
+        p = self.p
+        g = lambda k, d: params.get(k, d)
+        p.gamma = float(g("GAMMA", p.gamma))
+        p.p_max = float(g("P_MAX", p.p_max))
+        p.v_max = float(g("V_MAX", p.v_max))
+        p.limiter = _lib.LIMITER.get(str(g("LIMITER", "mc")).lower(), 0)
+        p.recon = _lib.RECON.get(str(g("RECON", "muscl")).lower(), 0)
+        r = str(g("RIEMANN", "hlle")).lower()
+        if self.physics == _lib.SRHD:
+            p.riemann = 1 if r == "hllc" else 0
+            # the reference's SRHD kernels take gamma as a default argument
+            # bound at import (srhd_core.py:47,62,134): always 5/3 unless the
+            # caller opts in to honouring GAMMA
+            p.srhd_gamma = p.gamma if g("SRHD_HONOUR_GAMMA", False) else 5.0 / 3.0
+        else:
+            p.riemann = 2 if r == "hlld_full" else (1 if r == "hlld" else 0)
+            p.glm_ch = float(g("GLM_CH", p.glm_ch))
+            p.glm_cp = float(g("GLM_CP", p.glm_cp))
+            p.resistive = 1 if g("RESISTIVE_ENABLED", bool(p.resistive)) else 0
+            p.resistivity = float(g("RESISTIVITY", p.resistivity))
+        p.n_passive = int(g("N_PASSIVE", p.n_passive))
+        p.passive_offset = int(g("PASSIVE_OFFSET", p.passive_offset))
+        fm = str(g("FLUX_MODE", "reference")).lower()
+        p.flux_mode = _lib.FLUX_CONSERVATIVE if fm == "conservative" else _lib.FLUX_REFERENCE
+        pm = str(g("PRECISION", "fp64")).lower()
+        p.precision = _lib.PREC_MIXED if pm == "mixed" else _lib.PREC_FP64
+        cg = str(g("C2P_GUESS", "reference")).lower()
+        p.c2p_guess = _lib.GUESS_LEARNED if cg == "learned" else _lib.GUESS_REFERENCE
+
+    # -- right-hand side --------------------------------------------------
+    def rhs(self, pr, nx, ny, nz, dx, dy, dz):
+        L = _lib.load()
+        t, was_np = rt.to_device(pr)
+        if tuple(t.shape[1:]) != (nx, ny, nz):
+            raise _lib.AstroError("nx, ny, nz must be the ghost-inclusive block extents")
+        grid = rt.grid_of(t, dx, dy, dz)
+        out = torch.empty((self.nm + self.p.n_passive, nx, ny, nz), dtype=torch.float64,
+                          device=t.device)
+        nb = L.astro_rhs_workspace_bytes(C.byref(self.p), C.byref(grid))
+        if nb == 0:
+            _lib.check(-2 if t.shape[0] < self.nm else -4, "astro_rhs (configuration)")
+        w = rt.workspace(nb, t.device)
+        _lib.check(L.astro_rhs(C.byref(self.p), C.byref(grid), rt.ptr(t), rt.ptr(out),
+                               rt.ptr(w), nb, rt.stream_handle(t.device)), "astro_rhs")
+        return out.cpu().numpy() if was_np else out
+
+    # -- one SSPRK step ---------------------------------------------------
+    def step(self, pr, dx, dy, dz, dt, rk_order, out=None):
+        L = _lib.load()
+        t, was_np = rt.to_device(pr)
+        grid = rt.grid_of(t, dx, dy, dz)
+        if out is None:
+            out = torch.empty_like(t)
+        nb = L.astro_step_workspace_bytes(C.byref(self.p), C.byref(grid))
+        if nb == 0:
+            _lib.check(-4, "astro_step (configuration)")
+        w = rt.workspace(nb, t.device)
+        stats = self._stats_buffer(t.device)
+        _lib.check(L.astro_step(C.byref(self.p), C.byref(grid), rt.ptr(t), rt.ptr(out),
+                                float(dt), int(rk_order), rt.ptr(w), nb, rt.ptr(stats),
+                                rt.stream_handle(t.device)), "astro_step")
+        return out.cpu().numpy() if was_np else out
+
+    def step_profiled(self, pr, dx, dy, dz, dt, rk_order, out):
+        """One step with per-kernel-class CUDA-event times (synchronises)."""
+        L = _lib.load()
+        grid = rt.grid_of(pr, dx, dy, dz)
+        nb = L.astro_step_workspace_bytes(C.byref(self.p), C.byref(grid))
+        w = rt.workspace(nb, pr.device)
+        stats = self._stats_buffer(pr.device)
+        times = _lib.AstroKernelTimes()
+        _lib.check(L.astro_step_profiled(C.byref(self.p), C.byref(grid), rt.ptr(pr), rt.ptr(out),
+                                         float(dt), int(rk_order), rt.ptr(w), nb, rt.ptr(stats),
+                                         rt.stream_handle(pr.device), C.byref(times)),
+                   "astro_step_profiled")
+        return out, [times.ms[i] for i in range(4)], [times.launches[i] for i in range(4)]
+
+    def _stats_buffer(self, device):
+        if self.stats is None or self.stats.device != torch.device(device):
+            self.stats = torch.zeros(8, dtype=torch.int64, device=device)
+        return self.stats
+
+    def c2p_stats(self, reset=False):
+        """con2prim outcome counters accumulated since the last reset."""
+        if self.stats is None:
+            return {}
+        v = self.stats.cpu().tolist()
+        names = [f for f, _ in _lib.AstroC2PStats._fields_]
+        if reset:
+            self.stats.zero_()
+        return dict(zip(names, v))
+
+    # -- CFL ---------------------------------------------------------------
+    def max_char_speed(self, pr, nx, ny, nz):
+        L = _lib.load()
+        t, _ = rt.to_device(pr)
+        grid = rt.grid_of(t)
+        out = torch.empty(1, dtype=torch.float64, device=t.device)
+        _lib.check(L.astro_max_char_speed(C.byref(self.p), C.byref(grid), rt.ptr(t), rt.ptr(out),
+                                          None, 0, rt.stream_handle(t.device)),
+                   "astro_max_char_speed")
+        return out
+
+    # -- pointwise conversions ----------------------------------------------
+    def p2c_array(self, q):
+        L = _lib.load()
+        t, was_np = rt.to_device(q)
+        t = t.reshape(self.nm, -1).contiguous()
+        out = torch.empty_like(t)
+        _lib.check(L.astro_p2c(C.byref(self.p), rt.ptr(t), rt.ptr(out), t.shape[1],
+                               rt.stream_handle(t.device)), "astro_p2c")
+        return out.cpu().numpy() if was_np else out
+
+    def c2p_array(self, U):
+        L = _lib.load()
+        t, was_np = rt.to_device(U)
+        t = t.reshape(self.nm, -1).contiguous()
+        out = torch.empty_like(t)
+        stats = self._stats_buffer(t.device)
+        _lib.check(L.astro_c2p(C.byref(self.p), rt.ptr(t), rt.ptr(out), t.shape[1],
+                               rt.ptr(stats), rt.stream_handle(t.device)), "astro_c2p")
+        return out.cpu().numpy() if was_np else out
+
+    def scalar_convert(self, fn, values):
+        """Scalar call (the reference's per-cell helpers): routed through the
+        same device kernels on a one-element batch."""
+        a = np.asarray(values, dtype=np.float64).reshape(self.nm, -1)
+        if a.shape[1] != 1:
+            return fn(a)
+        res = fn(a)
+        res = res.cpu().numpy() if isinstance(res, torch.Tensor) else res
+        return tuple(float(x) for x in res[:, 0])

@@ -1,0 +1,944 @@
+// kernels.cu -- sm_100a kernels and the C ABI of libastrofd_b200.so.
+//
+// Per SSPRK stage the right-hand side is built face by face:
+//   k_face    one thread per cell face in one direction: reconstruct the
+//             left/right primitive states from the 4- or 6-point stencil,
+//             floor, p2c, physical flux, wave speeds, Riemann flux.  Every face
+//             is evaluated once (the reference evaluates each face twice, once
+//             from each neighbour).  The result lands in a per-direction face
+//             buffer F[v][cell], indexed by the cell on the high side.
+//   k_update  one thread per cell (ghosts included): flux divergence, GLM
+//             damping, resistive Laplacian, passive-scalar fluxes, the SSPRK
+//             combination in float64 and con2prim, writing U_k and the next
+//             stage's primitives.  Cells outside the reference's loop bounds get
+//             rhs = 0, i.e. the reference's p2c -> c2p round trip.
+// The reference's RMHD PPM/WENO x faces use the wave speeds left over from the
+// previous cell's z face (core/rmhd_core.py:1285,1314,1445,1468).  In
+// ASTRO_FLUX_REFERENCE mode those faces are evaluated a second time with the
+// carried speeds (k_face<GIVEN=true>), read from the z-face speed buffer; in
+// ASTRO_FLUX_CONSERVATIVE mode every face uses its own speeds, so each face
+// flux enters both neighbours and the scheme conserves D, S, tau exactly.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <atomic>
+
+#include "physics.cuh"
+
+using namespace astro;
+
+namespace {
+
+// process-wide count of kernels this library has launched (diagnostic only)
+std::atomic<unsigned long long> g_launches{0};
+
+// Optional per-launch CUDA-event timing used by astro_step_profiled: an event
+// is recorded after every launch; the gap to the previous event is charged to
+// the launch's kernel class.
+struct Prof {
+    static constexpr int kMax = 64;
+    cudaEvent_t ev[kMax + 1];
+    int kind[kMax];
+    int n = 0;
+    bool on = false;
+};
+thread_local Prof* t_prof = nullptr;
+
+inline void mark(int kind, cudaStream_t s) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    Prof* P = t_prof;
+    if (P && P->on && P->n < Prof::kMax) {
+        cudaEventRecord(P->ev[P->n + 1], s);
+        P->kind[P->n++] = kind;
+    }
+}
+
+constexpr int kMaxPassive = 8;
+constexpr int kMaxNV = 64;
+
+struct Bounds {
+    int lo, hi[3];  // cells updated: [lo, hi[d]) per dimension
+};
+
+// loop bounds of the reference right-hand sides (ghost-inclusive indices)
+__host__ Bounds bounds_of(const AstroParams& p, const AstroGrid& g) {
+    Bounds b;
+    b.lo = (p.recon == ASTRO_RECON_MUSCL) ? 2 : 3;
+    int off = (p.recon != ASTRO_RECON_MUSCL) ? 3 : (p.physics == ASTRO_SRHD ? 3 : 2);
+    b.hi[0] = g.nx - off;
+    b.hi[1] = g.ny - off;
+    b.hi[2] = g.nz - off;
+    return b;
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Layout {
+    size_t prA, prB, U, F[3], FxC, aux[3], Sz, total;
+};
+
+inline bool carried_mode(const AstroParams& p) {
+    return p.physics == ASTRO_RMHD && p.recon != ASTRO_RECON_MUSCL &&
+           p.flux_mode == ASTRO_FLUX_REFERENCE;
+}
+
+inline bool passive_fluxes(const AstroParams& p) {
+    if (p.n_passive <= 0) return false;
+    if (p.physics == ASTRO_SRHD) return p.recon != ASTRO_RECON_WENO;
+    return p.recon == ASTRO_RECON_MUSCL;
+}
+
+Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
+    Layout L;
+    const size_t nc = (size_t)g.nx * g.ny * g.nz;
+    const int nm = p.physics == ASTRO_SRHD ? 5 : 9;
+    const size_t rs = p.precision == ASTRO_PREC_MIXED ? 4 : 8;
+    size_t o = 0;
+    auto take = [&](size_t bytes) { size_t r = o; o += align256(bytes); return r; };
+    L.prA = with_state ? take((size_t)g.nv * nc * 8) : 0;
+    L.prB = with_state ? take((size_t)g.nv * nc * 8) : 0;
+    L.U = with_state ? take((size_t)nm * nc * 8) : 0;
+    for (int d = 0; d < 3; ++d) L.F[d] = take((size_t)nm * nc * rs);
+    L.FxC = carried_mode(p) ? take((size_t)nm * nc * rs) : 0;
+    for (int d = 0; d < 3; ++d) L.aux[d] = passive_fluxes(p) ? take(4 * nc * rs) : 0;
+    L.Sz = carried_mode(p) ? take(2 * nc * rs) : 0;
+    L.total = o;
+    return L;
+}
+
+int validate(const AstroParams* p, const AstroGrid* g) {
+    if (!p || !g) return ASTRO_E_INVALID;
+    if (p->physics != ASTRO_SRHD && p->physics != ASTRO_RMHD) return ASTRO_E_INVALID;
+    if (p->recon < 0 || p->recon > 2 || p->limiter < 0 || p->limiter > 2) return ASTRO_E_INVALID;
+    if (p->riemann < 0 || p->riemann > (p->physics == ASTRO_SRHD ? 1 : 2)) return ASTRO_E_INVALID;
+    if (p->precision != ASTRO_PREC_FP64 && p->precision != ASTRO_PREC_MIXED) return ASTRO_E_INVALID;
+    if (p->flux_mode != ASTRO_FLUX_REFERENCE && p->flux_mode != ASTRO_FLUX_CONSERVATIVE)
+        return ASTRO_E_INVALID;
+    const int nm = p->physics == ASTRO_SRHD ? 5 : 9;
+    if (g->nv < nm || g->nv > kMaxNV) return ASTRO_E_SHAPE;
+    if (p->n_passive < 0 || p->n_passive > kMaxPassive) return ASTRO_E_UNSUPPORTED;
+    if (p->n_passive > 0 && (p->passive_offset < nm || p->passive_offset + p->n_passive > g->nv))
+        return ASTRO_E_SHAPE;
+    // SRHD blocks of 15+ variables carry Israel-Stewart dissipation fields whose
+    // fluxes (srhd_core.py:394-462) are outside this library's scope.
+    if (p->physics == ASTRO_SRHD && (g->nv >= 15 || (p->n_passive > 0 && p->passive_offset != 5)))
+        return ASTRO_E_UNSUPPORTED;
+    if (g->nx < 8 || g->ny < 8 || g->nz < 8) return ASTRO_E_SHAPE;
+    if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0)) return ASTRO_E_INVALID;
+    return ASTRO_OK;
+}
+
+// ------------------------------------------------------------ face pass ---
+struct FaceArgs {
+    const double* pr;
+    int nx, ny, nz;
+    int dir;
+    int org[3], ext[3];  // first cell and extents of the face block
+    Bounds b;
+    void* F;             // R[nm][nc]
+    void* aux;           // R[4][nc]: sL, sR, vL, vR (or null)
+    void* speeds_out;    // R[2][nc]: sL, sR (z faces, carried mode) or null
+    const void* carried; // R[2][nc]: z-face speeds read by the carried x faces
+    AstroParams p;
+};
+
+template <int PHYS, int RECON, int RIEMANN, typename R, bool GIVEN>
+__global__ void __launch_bounds__(128) k_face(FaceArgs a) {
+    constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
+    const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int c = (int)(t % a.ext[2]);
+    const long r = t / a.ext[2];
+    const int bb = (int)(r % a.ext[1]);
+    const int aa = (int)(r / a.ext[1]);
+    const int i = a.org[0] + aa, j = a.org[1] + bb, k = a.org[2] + c;
+    const size_t nc = (size_t)a.nx * a.ny * a.nz;
+    const size_t cell = ((size_t)i * a.ny + j) * a.nz + k;
+    const long stride = a.dir == 0 ? (long)a.ny * a.nz : (a.dir == 1 ? (long)a.nz : 1L);
+    const Phys<R> P = Phys<R>::from(a.p);
+
+    R qL[NM], qR[NM];
+    constexpr int o0 = RECON == ASTRO_RECON_MUSCL ? -2 : -3;
+    constexpr int o1 = RECON == ASTRO_RECON_MUSCL ? 1 : 2;
+#pragma unroll
+    for (int v = 0; v < NM; ++v) {
+        R s[6];
+        const double* base = a.pr + (size_t)v * nc + cell;
+#pragma unroll
+        for (int o = o0; o <= o1; ++o) s[o + 3] = (R)__ldg(base + o * stride);
+        recon_face<RECON>(s, a.p.limiter, qL[v], qR[v]);
+    }
+    R F[NM];
+    R sL = R(-1), sR = R(1);
+    if (GIVEN) {
+        // previous cell of the reference's i-j-k loop, whose z-low face speeds
+        // are still in (sL, sR) when this cell's x-low face is evaluated
+        int pi = i, pj = j, pk = k;
+        bool first = false;
+        if (k > a.b.lo) pk = k - 1;
+        else if (j > a.b.lo) { pj = j - 1; pk = a.b.hi[2] - 1; }
+        else if (i > a.b.lo) { pi = i - 1; pj = a.b.hi[1] - 1; pk = a.b.hi[2] - 1; }
+        else first = true;
+        if (!first) {
+            const R* S = (const R*)a.carried;
+            const size_t pc = ((size_t)pi * a.ny + pj) * a.nz + pk;
+            sL = S[pc];
+            sR = S[nc + pc];
+        }
+    }
+    if (PHYS == ASTRO_SRHD) {
+        s_face<RIEMANN>(P, a.dir, qL, qR, F, sL, sR);
+    } else {
+        r_face<RIEMANN, RECON == ASTRO_RECON_MUSCL, GIVEN>(P, a.dir, qL, qR, F, sL, sR);
+    }
+    R* Fo = (R*)a.F;
+#pragma unroll
+    for (int v = 0; v < NM; ++v) Fo[(size_t)v * nc + cell] = F[v];
+    if (a.aux) {
+        R* A = (R*)a.aux;
+        A[cell] = sL;
+        A[nc + cell] = sR;
+        A[2 * nc + cell] = qL[1 + a.dir];
+        A[3 * nc + cell] = qR[1 + a.dir];
+    }
+    if (a.speeds_out) {
+        R* S = (R*)a.speeds_out;
+        S[cell] = sL;
+        S[nc + cell] = sR;
+    }
+}
+
+// ---------------------------------------------------------- update pass ---
+struct UpdArgs {
+    const double* pr0;   // step input primitives (U0 = p2c(pr0), passives t0)
+    const double* prk;   // this stage's input primitives
+    double* U;           // U_{k-1} in, U_k out (may be null for rhs-only)
+    double* dst;         // next primitives (stage mode) or rhs (rhs mode)
+    const void* F[3];
+    const void* FxL;     // x-low-face fluxes (== F[0] unless carried mode)
+    const void* aux[3];
+    int nv, nx, ny, nz;
+    Bounds b;
+    double dd[3], dt;
+    int stage, nstages, rhs_only;
+    AstroParams p;
+    AstroC2PStats* stats;
+};
+
+// Numba's addressing for the passive stencils of the MUSCL right-hand sides:
+// negative indices wrap per axis, positive overruns alias the next row of the
+// C-contiguous block (core/srhd_core.py:550-560, core/rmhd_core.py:832-940).
+// A read past the end of the block is undefined in the reference; NaN here.
+__device__ __forceinline__ double pget(const double* pr, int nv, int nx, int ny, int nz, int v,
+                                       int i, int j, int k) {
+    if (i < 0) i += nx;
+    if (j < 0) j += ny;
+    if (k < 0) k += nz;
+    const size_t flat = (((size_t)v * nx + i) * ny + j) * nz + k;
+    if (flat >= (size_t)nv * nx * ny * nz) return __longlong_as_double(0x7ff8000000000000LL);
+    return __ldg(pr + flat);
+}
+
+enum { PK_WENO = 0, PK_PPM = 1, PK_MC = 2 };
+
+__device__ double passive_face(const UpdArgs& a, int idx, int kind, int n, int i, int j, int k,
+                               double vL, double vR, double sL, double sR) {
+    const int di = n == 0, dj = n == 1, dk = n == 2;
+    double s[6];
+#pragma unroll
+    for (int o = -3; o <= 2; ++o)
+        s[o + 3] = pget(a.prk, a.nv, a.nx, a.ny, a.nz, idx, i + o * di, j + o * dj, k + o * dk);
+    double tL, tR;
+    if (kind == PK_WENO) recon_face<ASTRO_RECON_WENO>(s, 0, tL, tR);
+    else if (kind == PK_PPM) recon_face<ASTRO_RECON_PPM>(s, 0, tL, tR);
+    else recon_face<ASTRO_RECON_MUSCL>(s, a.p.limiter, tL, tR);
+    return hlle_scalar(tL, tR, tL * vL, tR * vR, sL, sR);
+}
+
+template <typename RF> __device__ __forceinline__ double ldf(const void* p, size_t i) {
+    return (double)__ldg((const RF*)p + i);
+}
+
+template <int PHYS, typename RF>
+__global__ void __launch_bounds__(128) k_update(UpdArgs a) {
+    constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
+    const size_t nc = (size_t)a.nx * a.ny * a.nz;
+    const size_t cell = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    C2PCount cnt;
+    if (cell < nc) {
+        const int k = (int)(cell % a.nz);
+        const int j = (int)((cell / a.nz) % a.ny);
+        const int i = (int)(cell / ((size_t)a.nz * a.ny));
+        const bool in = i >= a.b.lo && i < a.b.hi[0] && j >= a.b.lo && j < a.b.hi[1] &&
+                        k >= a.b.lo && k < a.b.hi[2];
+        const long st[3] = {(long)a.ny * a.nz, (long)a.nz, 1L};
+        const int np = a.p.n_passive, po = a.p.passive_offset;
+        double rhs[NM];
+        double rp[kMaxPassive];
+#pragma unroll
+        for (int v = 0; v < NM; ++v) rhs[v] = 0.0;
+        for (int t = 0; t < np; ++t) rp[t] = 0.0;
+        if (in) {
+#pragma unroll
+            for (int v = 0; v < NM; ++v) {
+                const size_t o = (size_t)v * nc + cell;
+                double r = 0.0;
+                r -= (ldf<RF>(a.F[0], o + st[0]) - ldf<RF>(a.FxL, o)) / a.dd[0];
+                r -= (ldf<RF>(a.F[1], o + st[1]) - ldf<RF>(a.F[1], o)) / a.dd[1];
+                r -= (ldf<RF>(a.F[2], o + st[2]) - ldf<RF>(a.F[2], o)) / a.dd[2];
+                rhs[v] = r;
+            }
+            if (PHYS == ASTRO_RMHD) {
+                const double* q = a.prk;
+                rhs[8] -= a.p.glm_cp * a.p.glm_cp * q[8 * nc + cell];
+                int nres = (a.p.resistive && a.p.resistivity > 0.0)
+                               ? (a.p.recon == ASTRO_RECON_MUSCL ? 1 : (a.p.recon == ASTRO_RECON_PPM ? 2 : 0))
+                               : 0;
+                // conservative mode applies eta*Laplacian(B) exactly once for
+                // every reconstruction (the reference adds it twice for PPM and
+                // not at all for WENO, rmhd_core.py:1414-1435,1440-1557)
+                if (a.p.flux_mode == ASTRO_FLUX_CONSERVATIVE)
+                    nres = (a.p.resistive && a.p.resistivity > 0.0) ? 1 : 0;
+                for (int rep = 0; rep < nres; ++rep) {
+                    const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
+                    const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
+                    const double iz2 = 1.0 / (a.dd[2] * a.dd[2] + 1e-12);
+#pragma unroll
+                    for (int c = 5; c < 8; ++c) {
+                        const double* B = q + (size_t)c * nc + cell;
+                        double lap = (B[st[0]] - 2.0 * B[0] + B[-st[0]]) * ix2 +
+                                     (B[st[1]] - 2.0 * B[0] + B[-st[1]]) * iy2 +
+                                     (B[st[2]] - 2.0 * B[0] + B[-st[2]]) * iz2;
+                        rhs[c] += a.p.resistivity * lap;
+                    }
+                }
+            }
+            // passive scalars: the reference's triple evaluation (see header)
+            if (np > 0) {
+                for (int n = 0; n < 3; ++n) {
+                    int kinds[3], nk = 0, lkind = PK_MC;
+                    if (PHYS == ASTRO_SRHD) {
+                        if (a.p.recon == ASTRO_RECON_MUSCL && n == 0) { kinds[0] = PK_WENO; kinds[1] = PK_PPM; kinds[2] = PK_MC; nk = 3; }
+                        if (a.p.recon == ASTRO_RECON_MUSCL && n == 2) { kinds[0] = PK_MC; nk = 1; }
+                        if (a.p.recon == ASTRO_RECON_PPM && n == 1) { kinds[0] = PK_WENO; kinds[1] = PK_PPM; kinds[2] = PK_MC; nk = 3; }
+                        if (a.p.recon == ASTRO_RECON_PPM && n == 2) { kinds[0] = PK_WENO; kinds[1] = PK_PPM; nk = 2; lkind = PK_PPM; }
+                    } else if (a.p.recon == ASTRO_RECON_MUSCL) {
+                        kinds[0] = PK_WENO; kinds[1] = PK_PPM; kinds[2] = PK_MC; nk = 3;
+                    }
+                    if (nk == 0) continue;
+                    const size_t lo = cell, hi = cell + st[n];
+                    const double sLl = ldf<RF>(a.aux[n], lo), sRl = ldf<RF>(a.aux[n], nc + lo);
+                    const double vLl = ldf<RF>(a.aux[n], 2 * nc + lo), vRl = ldf<RF>(a.aux[n], 3 * nc + lo);
+                    double sLh = ldf<RF>(a.aux[n], hi), sRh = ldf<RF>(a.aux[n], nc + hi);
+                    const double vLh = ldf<RF>(a.aux[n], 2 * nc + hi), vRh = ldf<RF>(a.aux[n], 3 * nc + hi);
+                    if (PHYS == ASTRO_RMHD) { sLh = sLl; sRh = sRl; }  // low-face speeds reused
+                    const int i2 = i + (n == 0), j2 = j + (n == 1), k2 = k + (n == 2);
+                    for (int t = 0; t < np; ++t) {
+                        const int idx = po + t;
+                        const double FLt = passive_face(a, idx, lkind, n, i, j, k, vLl, vRl, sLl, sRl);
+                        double acc = 0.0;
+                        for (int q = 0; q < nk; ++q) {
+                            const double FRt = passive_face(a, idx, kinds[q], n, i2, j2, k2, vLh, vRh, sLh, sRh);
+                            acc -= (FRt - FLt) / a.dd[n];
+                        }
+                        rp[t] += acc;
+                    }
+                }
+            }
+        }
+        if (a.rhs_only) {
+#pragma unroll
+            for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = rhs[v];
+            for (int t = 0; t < np; ++t) a.dst[(size_t)(NM + t) * nc + cell] = rp[t];
+        } else {
+            const Phys<double> P = Phys<double>::from(a.p);
+            double q0[NM], U0[NM], Un[NM], q[NM];
+#pragma unroll
+            for (int v = 0; v < NM; ++v) q0[v] = a.pr0[(size_t)v * nc + cell];
+            if (PHYS == ASTRO_SRHD) s_p2c(P, q0, U0);
+            else r_p2c(P, q0, U0);
+            const double dt = a.dt;
+#pragma unroll
+            for (int v = 0; v < NM; ++v) {
+                const double r = rhs[v], u0 = U0[v];
+                double un;
+                if (a.stage == 0) un = __dadd_rn(u0, __dmul_rn(dt, r));
+                else {
+                    const double uk = a.U[(size_t)v * nc + cell];
+                    if (a.nstages == 2)
+                        un = __dmul_rn(0.5, __dadd_rn(__dadd_rn(u0, uk), __dmul_rn(dt, r)));
+                    else if (a.stage == 1)
+                        un = __dadd_rn(__dmul_rn(0.75, u0), __dmul_rn(0.25, __dadd_rn(uk, __dmul_rn(dt, r))));
+                    else
+                        un = __dadd_rn(__dmul_rn(1.0 / 3.0, u0),
+                                       __dmul_rn(2.0 / 3.0, __dadd_rn(uk, __dmul_rn(dt, r))));
+                }
+                Un[v] = un;
+            }
+            if (a.stage != a.nstages - 1) {
+#pragma unroll
+                for (int v = 0; v < NM; ++v) a.U[(size_t)v * nc + cell] = Un[v];
+            }
+            if (PHYS == ASTRO_SRHD) s_c2p(P, Un, q);
+            else r_c2p(P, Un, q, cnt);
+#pragma unroll
+            for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = q[v];
+            for (int v = NM; v < a.nv; ++v) {
+                double out = 0.0;
+                const int t = v - po;
+                if (np > 0 && t >= 0 && t < np) {
+                    const size_t o = (size_t)v * nc + cell;
+                    const double t0 = a.pr0[o], r = rp[t];
+                    if (a.stage == 0) out = __dadd_rn(t0, __dmul_rn(dt, r));
+                    else {
+                        const double tk = a.prk[o];
+                        if (a.nstages == 2)
+                            out = __dmul_rn(0.5, __dadd_rn(__dadd_rn(t0, tk), __dmul_rn(dt, r)));
+                        else if (a.stage == 1)
+                            out = __dadd_rn(__dmul_rn(0.75, t0), __dmul_rn(0.25, __dadd_rn(tk, __dmul_rn(dt, r))));
+                        else
+                            out = __dadd_rn(__dmul_rn(1.0 / 3.0, t0),
+                                            __dmul_rn(2.0 / 3.0, __dadd_rn(tk, __dmul_rn(dt, r))));
+                    }
+                }
+                a.dst[(size_t)v * nc + cell] = out;
+            }
+        }
+    }
+    if (a.stats && !a.rhs_only) {
+        // warp-aggregated counters, one atomic per warp and counter
+        unsigned n1 = __reduce_add_sync(0xffffffffu, cell < nc ? 1u : 0u);
+        unsigned n2 = __reduce_add_sync(0xffffffffu, cnt.newton);
+        unsigned n3 = __reduce_add_sync(0xffffffffu, cnt.bisect);
+        unsigned n4 = __reduce_add_sync(0xffffffffu, cnt.hydro_fallback);
+        if ((threadIdx.x & 31) == 0) {
+            if (n1) atomicAdd(&a.stats->cells, (unsigned long long)n1);
+            if (n2) atomicAdd(&a.stats->newton, (unsigned long long)n2);
+            if (n3) atomicAdd(&a.stats->bisection, (unsigned long long)n3);
+            if (n4) atomicAdd(&a.stats->hydro_fallback, (unsigned long long)n4);
+        }
+    }
+}
+
+// ------------------------------------------------------------- dispatch ---
+template <typename R>
+cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
+    const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
+    if (total <= 0) return cudaSuccess;
+    const dim3 blk(128), grd((unsigned)((total + 127) / 128));
+    const AstroParams& p = a.p;
+#define FACE(PH, RE, RI)                                                        \
+    do {                                                                        \
+        if (given) k_face<PH, RE, RI, R, true><<<grd, blk, 0, s>>>(a);          \
+        else k_face<PH, RE, RI, R, false><<<grd, blk, 0, s>>>(a);               \
+    } while (0)
+#define RECONS(PH, RI)                                                          \
+    do {                                                                        \
+        if (p.recon == 0) FACE(PH, 0, RI);                                      \
+        else if (p.recon == 1) FACE(PH, 1, RI);                                 \
+        else FACE(PH, 2, RI);                                                   \
+    } while (0)
+    if (p.physics == ASTRO_SRHD) {
+        if (p.riemann == 1) RECONS(ASTRO_SRHD, 1);
+        else RECONS(ASTRO_SRHD, 0);
+    } else {
+        if (p.riemann == 2) RECONS(ASTRO_RMHD, 2);
+        else if (p.riemann == 1) RECONS(ASTRO_RMHD, 1);
+        else RECONS(ASTRO_RMHD, 0);
+    }
+#undef RECONS
+#undef FACE
+    mark(0, s);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
+    const size_t nc = (size_t)a.nx * a.ny * a.nz;
+    const dim3 blk(128), grd((unsigned)((nc + 127) / 128));
+    const bool mixed = a.p.precision == ASTRO_PREC_MIXED;
+    if (a.p.physics == ASTRO_SRHD) {
+        if (mixed) k_update<ASTRO_SRHD, float><<<grd, blk, 0, s>>>(a);
+        else k_update<ASTRO_SRHD, double><<<grd, blk, 0, s>>>(a);
+    } else {
+        if (mixed) k_update<ASTRO_RMHD, float><<<grd, blk, 0, s>>>(a);
+        else k_update<ASTRO_RMHD, double><<<grd, blk, 0, s>>>(a);
+    }
+    mark(1, s);
+    return cudaGetLastError();
+}
+
+// All face passes of one stage: z (with speeds in carried mode), x, carried x, y.
+cudaError_t face_passes(const AstroParams& p, const AstroGrid& g, const Bounds& b,
+                        const double* pr, char* work, const Layout& L, cudaStream_t s) {
+    const bool carried = carried_mode(p);
+    const bool mixed = p.precision == ASTRO_PREC_MIXED;
+    const int order[3] = {2, 0, 1};
+    for (int oi = 0; oi < 3; ++oi) {
+        const int d = order[oi];
+        FaceArgs a;
+        memset(&a, 0, sizeof(a));
+        a.pr = pr; a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.dir = d; a.b = b; a.p = p;
+        for (int e = 0; e < 3; ++e) {
+            a.org[e] = b.lo;
+            a.ext[e] = b.hi[e] - b.lo + (e == d ? 1 : 0);
+        }
+        a.F = work + L.F[d];
+        a.aux = passive_fluxes(p) ? (void*)(work + L.aux[d]) : nullptr;
+        a.speeds_out = (carried && d == 2) ? (void*)(work + L.Sz) : nullptr;
+        cudaError_t e = mixed ? launch_face_t<float>(a, false, s) : launch_face_t<double>(a, false, s);
+        if (e != cudaSuccess) return e;
+        if (carried && d == 0) {
+            FaceArgs c = a;
+            c.ext[0] = b.hi[0] - b.lo;  // x-low faces of the updated cells
+            c.F = work + L.FxC;
+            c.aux = nullptr;
+            c.speeds_out = nullptr;
+            c.carried = work + L.Sz;
+            e = mixed ? launch_face_t<float>(c, true, s) : launch_face_t<double>(c, true, s);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    return cudaSuccess;
+}
+
+UpdArgs update_args(const AstroParams& p, const AstroGrid& g, const Bounds& b, char* work,
+                    const Layout& L) {
+    UpdArgs u;
+    memset(&u, 0, sizeof(u));
+    for (int d = 0; d < 3; ++d) {
+        u.F[d] = work + L.F[d];
+        u.aux[d] = passive_fluxes(p) ? (const void*)(work + L.aux[d]) : nullptr;
+    }
+    u.FxL = carried_mode(p) ? (const void*)(work + L.FxC) : u.F[0];
+    u.nv = g.nv; u.nx = g.nx; u.ny = g.ny; u.nz = g.nz;
+    u.b = b;
+    u.dd[0] = g.dx; u.dd[1] = g.dy; u.dd[2] = g.dz;
+    u.p = p;
+    return u;
+}
+
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? ASTRO_OK : ASTRO_E_CUDA; }
+
+// ------------------------------------------------------- CFL reduction ---
+__global__ void k_max_char_speed(const double* pr, int nx, int ny, int nz, double srhd_gamma,
+                                 unsigned long long* out) {
+    const size_t n = (size_t)(nx - 2) * (ny - 2) * (nz - 2);
+    const size_t nc = (size_t)nx * ny * nz;
+    Phys<double> P;
+    P.srhd_gamma = srhd_gamma;
+    double loc = 0.0;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = 1 + (int)(t % (nz - 2));
+        const int j = 1 + (int)((t / (nz - 2)) % (ny - 2));
+        const int i = 1 + (int)(t / ((size_t)(nz - 2) * (ny - 2)));
+        const size_t c = ((size_t)i * ny + j) * nz + k;
+        const double cs = s_sound_speed(P, pr[c], pr[4 * nc + c]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double lm, lp;
+            eig_speeds(pr[(1 + d) * nc + c], cs, lm, lp);
+            loc = rmax(loc, rmax(fabs(lm), fabs(lp)));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loc = rmax(loc, __shfl_xor_sync(0xffffffffu, loc, o));
+    __shared__ double wmax[32];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = loc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double v = threadIdx.x < (blockDim.x >> 5) ? wmax[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = rmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        // non-negative doubles order like their bit patterns
+        if (threadIdx.x == 0) atomicMax(out, (unsigned long long)__double_as_longlong(v));
+    }
+}
+
+__global__ void k_floor_small(double* out) {
+    if (*out < 1e-12) *out = 1e-12;
+}
+
+// ------------------------------------------------------------ ghosts -----
+__global__ void k_periodic_yz(double* pr, int nv, int nx, int ny, int nz, int ng) {
+    // every cell with a y or z ghost index receives orig[i, my(j), mz(k)];
+    // the sources all have interior j and k, so the gather is race free and
+    // equals the reference's sequential y-then-z slab copies
+    const size_t nc = (size_t)nx * ny * nz;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < nc;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t % nz);
+        const int j = (int)((t / nz) % ny);
+        const int i = (int)(t / ((size_t)nz * ny));
+        const bool gy = j < ng || j >= ny - ng, gz = k < ng || k >= nz - ng;
+        if (!gy && !gz) continue;
+        const int sj = j < ng ? j + (ny - 2 * ng) : (j >= ny - ng ? j - (ny - 2 * ng) : j);
+        const int sk = k < ng ? k + (nz - 2 * ng) : (k >= nz - ng ? k - (nz - 2 * ng) : k);
+        const size_t src = ((size_t)i * ny + sj) * nz + sk;
+        for (int v = 0; v < nv; ++v) pr[(size_t)v * nc + t] = pr[(size_t)v * nc + src];
+    }
+}
+
+__global__ void k_outflow_right_x(double* pr, int nv, int nx, int ny, int nz, int ng) {
+    const size_t plane = (size_t)ny * nz, nc = plane * nx;
+    const size_t n = plane * ng;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const size_t g = t / plane, jk = t % plane;
+        const size_t dst = (nx - ng + g) * plane + jk, src = (size_t)(nx - ng - 1) * plane + jk;
+        for (int v = 0; v < nv; ++v) pr[(size_t)v * nc + dst] = pr[(size_t)v * nc + src];
+    }
+}
+
+__device__ double nozzle_weight(double r, double radius, double shear, int profile) {
+    if (radius <= 0.0) return 0.0;
+    if (profile == 1) return r >= radius ? 0.0 : 0.5 * (1.0 + cos(M_PI * r / radius));
+    if (profile == 2) {
+        if (r >= radius) return 0.0;
+        double x = r / radius;
+        return rmax(0.0, 1.0 - x * x);
+    }
+    if (shear > 0.0) return 0.5 * (1.0 - tanh((r - radius) / shear));
+    return r <= radius ? 1.0 : 0.0;
+}
+
+__global__ void k_nozzle(double* pr, int nv, int nx, int ny, int nz, AstroNozzle c,
+                         const double* draws, const int32_t* rank_map, int n_weighted) {
+    const int ng = c.ng, nyl = ny - 2 * ng, nzl = nz - 2 * ng;
+    const size_t n = (size_t)ng * nyl * nzl, nc = (size_t)nx * ny * nz;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int kk = (int)(t % nzl), jj = (int)((t / nzl) % nyl), g = (int)(t / ((size_t)nzl * nyl));
+        const int j = jj + ng, k = kk + ng;
+        const double y = (j - ng + 0.5) * c.dy, z = (k - ng + 0.5) * c.dz;
+        const double rr = sqrt((y - c.y0) * (y - c.y0) + (z - c.z0) * (z - c.z0));
+        const double s = nozzle_weight(rr, c.radius, c.shear_thick, c.profile);
+        double rho = c.eta_rho * c.rho_amb * s + c.rho_amb * (1.0 - s);
+        double p = c.p_eq;
+        const double beta = sqrt(1.0 - 1.0 / (c.gamma_jet * c.gamma_jet));
+        double vx = beta * s + c.vx_amb * (1.0 - s);
+        double vy = c.vy_amb, vz = c.vz_amb;
+        // which cells draw random numbers is decided on the host with the
+        // reference's own Python math (the rank map), so the draw order and
+        // count match rng.random() calls in core/nozzle.py:50-53 exactly
+        if (c.perturb && draws && rank_map) {
+            const int rk = rank_map[(size_t)jj * nzl + kk];
+            if (rk >= 0) {
+                const double* d = draws + 3 * ((size_t)g * n_weighted + rk);
+                vy += c.turb_vamp * (2.0 * d[0] - 1.0);
+                vz += c.turb_vamp * (2.0 * d[1] - 1.0);
+                p *= (1.0 + c.turb_pamp * (2.0 * d[2] - 1.0));
+            }
+        }
+        const size_t cell = ((size_t)g * ny + j) * nz + k;
+        pr[cell] = rho;
+        pr[nc + cell] = vx;
+        pr[2 * nc + cell] = vy;
+        pr[3 * nc + cell] = vz;
+        pr[4 * nc + cell] = p;
+        if (nv >= 15)
+            for (int v = 5; v < 15; ++v) pr[(size_t)v * nc + cell] = 0.0;
+        for (int tt = 0; tt < c.n_tracers && tt < 8; ++tt) {
+            const double tn = c.tracer_nozzle[tt], ta = c.tracer_amb[tt];
+            pr[(size_t)(c.tracer_offset + tt) * nc + cell] = ta + (tn - ta) * s;
+        }
+        if (c.two_temperature && nv > c.thermo_offset + 1) {
+            pr[(size_t)c.thermo_offset * nc + cell] = c.te;
+            pr[(size_t)(c.thermo_offset + 1) * nc + cell] = c.ti;
+        }
+        if (c.physics == 1) {
+            double Bx = 0.0, By = 0.0;
+            if (c.b_init == 1) Bx = c.b0 * s;
+            else if (c.b_init == 2) By = c.b0 * s;
+            pr[5 * nc + cell] = Bx;
+            pr[6 * nc + cell] = By;
+            pr[7 * nc + cell] = 0.0;
+            pr[8 * nc + cell] = 0.0;
+        }
+    }
+}
+
+// -------------------------------------------------------- conversions ---
+__global__ void k_p2c(AstroParams p, const double* q, double* U, long count) {
+    const Phys<double> P = Phys<double>::from(p);
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long)gridDim.x * blockDim.x) {
+        double a[9], b[9];
+        const int nm = p.physics == ASTRO_SRHD ? 5 : 9;
+        for (int v = 0; v < nm; ++v) a[v] = q[(size_t)v * count + t];
+        if (p.physics == ASTRO_SRHD) s_p2c(P, a, b);
+        else r_p2c(P, a, b);
+        for (int v = 0; v < nm; ++v) U[(size_t)v * count + t] = b[v];
+    }
+}
+
+__global__ void k_c2p(AstroParams p, const double* U, double* q, long count, AstroC2PStats* stats) {
+    const Phys<double> P = Phys<double>::from(p);
+    C2PCount cnt;
+    unsigned mine = 0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long)gridDim.x * blockDim.x) {
+        double a[9], b[9];
+        const int nm = p.physics == ASTRO_SRHD ? 5 : 9;
+        for (int v = 0; v < nm; ++v) a[v] = U[(size_t)v * count + t];
+        if (p.physics == ASTRO_SRHD) s_c2p(P, a, b);
+        else r_c2p(P, a, b, cnt);
+        for (int v = 0; v < nm; ++v) q[(size_t)v * count + t] = b[v];
+        ++mine;
+    }
+    if (stats) {
+        atomicAdd(&stats->cells, (unsigned long long)mine);
+        if (cnt.newton) atomicAdd(&stats->newton, (unsigned long long)cnt.newton);
+        if (cnt.bisect) atomicAdd(&stats->bisection, (unsigned long long)cnt.bisect);
+        if (cnt.hydro_fallback) atomicAdd(&stats->hydro_fallback, (unsigned long long)cnt.hydro_fallback);
+    }
+}
+
+// ------------------------------------------------------------ sources ---
+__global__ void k_cooling(double* pr, int nx, int ny, int nz, int ng, double dt, double cool,
+                          double heat, double pmax) {
+    const size_t nc = (size_t)nx * ny * nz;
+    const int ex = nx - 2 * ng, ey = ny - 2 * ng, ez = nz - 2 * ng;
+    const size_t n = (size_t)ex * ey * ez;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = ng + (int)(t % ez), j = ng + (int)((t / ez) % ey), i = ng + (int)(t / ((size_t)ez * ey));
+        const size_t c = ((size_t)i * ny + j) * nz + k;
+        const double rho = pr[c], p = pr[4 * nc + c];
+        const double dp = __dmul_rn(dt, heat - __dmul_rn(__dmul_rn(cool, rho), p));
+        double pn = __dadd_rn(p, dp);
+        if (pn < 1e-12) pn = 1e-12;
+        if (pn > pmax) pn = pmax;
+        pr[4 * nc + c] = pn;
+    }
+}
+
+__global__ void k_two_temperature(double* pr, int nx, int ny, int nz, int ng, double dt,
+                                  double tau, int off) {
+    const size_t nc = (size_t)nx * ny * nz;
+    const int ex = nx - 2 * ng, ey = ny - 2 * ng, ez = nz - 2 * ng;
+    const size_t n = (size_t)ex * ey * ez;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = ng + (int)(t % ez), j = ng + (int)((t / ez) % ey), i = ng + (int)(t / ((size_t)ez * ey));
+        const size_t c = ((size_t)i * ny + j) * nz + k;
+        const double rho = pr[c], p = pr[4 * nc + c];
+        const double T = p / rmax(rho, 1e-12);
+        double Te = pr[(size_t)off * nc + c], Ti = pr[(size_t)(off + 1) * nc + c];
+        Te = __dadd_rn(Te, __dmul_rn(dt, T - Te) / tau);
+        Ti = __dadd_rn(Ti, __dmul_rn(dt, T - Ti) / tau);
+        pr[(size_t)off * nc + c] = Te;
+        pr[(size_t)(off + 1) * nc + c] = Ti;
+    }
+}
+
+int grid_for(size_t n, int block) {
+    size_t g = (n + block - 1) / block;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+// =================================================================== C ABI ==
+extern "C" {
+
+int astro_version(void) { return 10000; }
+
+const char* astro_error_string(int code) {
+    switch (code) {
+        case ASTRO_OK: return "ok";
+        case ASTRO_E_INVALID: return "invalid argument";
+        case ASTRO_E_SHAPE: return "grid shape incompatible with the stencil/ghost layers";
+        case ASTRO_E_WORKSPACE: return "workspace missing or too small";
+        case ASTRO_E_UNSUPPORTED: return "configuration not supported";
+        case ASTRO_E_CUDA: return "CUDA error";
+        default: return "unknown error";
+    }
+}
+
+size_t astro_rhs_workspace_bytes(const AstroParams* p, const AstroGrid* g) {
+    if (validate(p, g) != ASTRO_OK) return 0;
+    return layout_of(*p, *g, false).total;
+}
+
+int astro_rhs(const AstroParams* p, const AstroGrid* g, const double* pr, double* rhs,
+              void* work, size_t work_bytes, void* stream) {
+    int v = validate(p, g);
+    if (v != ASTRO_OK) return v;
+    if (!pr || !rhs) return ASTRO_E_INVALID;
+    const Layout L = layout_of(*p, *g, false);
+    if (!work || work_bytes < L.total) return ASTRO_E_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Bounds b = bounds_of(*p, *g);
+    cudaError_t e = face_passes(*p, *g, b, pr, (char*)work, L, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    UpdArgs u = update_args(*p, *g, b, (char*)work, L);
+    u.pr0 = pr; u.prk = pr; u.dst = rhs; u.rhs_only = 1;
+    return cuda_status(launch_update(u, s));
+}
+
+size_t astro_step_workspace_bytes(const AstroParams* p, const AstroGrid* g) {
+    if (validate(p, g) != ASTRO_OK) return 0;
+    return layout_of(*p, *g, true).total;
+}
+
+int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, double* pr_out,
+               double dt, int rk_order, void* work, size_t work_bytes, AstroC2PStats* stats,
+               void* stream) {
+    int v = validate(p, g);
+    if (v != ASTRO_OK) return v;
+    if (!pr_in || !pr_out || pr_in == pr_out) return ASTRO_E_INVALID;
+    if (rk_order != 2 && rk_order != 3) return ASTRO_E_INVALID;
+    if (p->c2p_guess != ASTRO_GUESS_REFERENCE) return ASTRO_E_UNSUPPORTED;
+    const Layout L = layout_of(*p, *g, true);
+    if (!work || work_bytes < L.total) return ASTRO_E_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* w = (char*)work;
+    const Bounds b = bounds_of(*p, *g);
+    const int nst = rk_order;
+    const double* cur = pr_in;
+    double* bufs[2] = {(double*)(w + L.prA), (double*)(w + L.prB)};
+    for (int st = 0; st < nst; ++st) {
+        cudaError_t e = face_passes(*p, *g, b, cur, w, L, s);
+        if (e != cudaSuccess) return ASTRO_E_CUDA;
+        double* dst = (st == nst - 1) ? pr_out : bufs[st % 2];
+        UpdArgs u = update_args(*p, *g, b, w, L);
+        u.pr0 = pr_in; u.prk = cur; u.U = (double*)(w + L.U); u.dst = dst;
+        u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
+        e = launch_update(u, s);
+        if (e != cudaSuccess) return ASTRO_E_CUDA;
+        cur = dst;
+    }
+    return ASTRO_OK;
+}
+
+unsigned long long astro_launch_count(void) { return g_launches.load(); }
+
+int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* pr_in,
+                        double* pr_out, double dt, int rk_order, void* work, size_t work_bytes,
+                        AstroC2PStats* stats, void* stream, AstroKernelTimes* times) {
+    if (!times) return ASTRO_E_INVALID;
+    Prof P;
+    for (int i = 0; i <= Prof::kMax; ++i)
+        if (cudaEventCreate(&P.ev[i]) != cudaSuccess) return ASTRO_E_CUDA;
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEventRecord(P.ev[0], s);
+    P.on = true;
+    t_prof = &P;
+    int rc = astro_step(p, g, pr_in, pr_out, dt, rk_order, work, work_bytes, stats, stream);
+    t_prof = nullptr;
+    if (rc == ASTRO_OK && cudaEventSynchronize(P.ev[P.n]) != cudaSuccess) rc = ASTRO_E_CUDA;
+    memset(times, 0, sizeof(*times));
+    if (rc == ASTRO_OK) {
+        for (int i = 0; i < P.n; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, P.ev[i], P.ev[i + 1]);
+            const int k = P.kind[i] < 4 ? P.kind[i] : 3;
+            times->ms[k] += ms;
+            times->launches[k] += 1;
+        }
+    }
+    for (int i = 0; i <= Prof::kMax; ++i) cudaEventDestroy(P.ev[i]);
+    return rc;
+}
+
+size_t astro_max_char_speed_workspace_bytes(void) { return 0; }
+
+int astro_max_char_speed(const AstroParams* p, const AstroGrid* g, const double* pr,
+                         double* out, void* work, size_t work_bytes, void* stream) {
+    (void)work; (void)work_bytes;
+    if (!p || !g || !pr || !out) return ASTRO_E_INVALID;
+    if (g->nv < 5 || g->nx < 3 || g->ny < 3 || g->nz < 3) return ASTRO_E_SHAPE;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(out, 0, sizeof(double), s) != cudaSuccess) return ASTRO_E_CUDA;
+    const size_t n = (size_t)(g->nx - 2) * (g->ny - 2) * (g->nz - 2);
+    k_max_char_speed<<<grid_for(n, 256), 256, 0, s>>>(pr, g->nx, g->ny, g->nz, p->srhd_gamma,
+                                                     (unsigned long long*)out);
+    mark(2, s);
+    k_floor_small<<<1, 1, 0, s>>>(out);
+    mark(2, s);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_periodic_yz(double* pr, const AstroGrid* g, int ng, void* stream) {
+    if (!pr || !g || ng < 1) return ASTRO_E_INVALID;
+    if (g->ny - 2 * ng < ng || g->nz - 2 * ng < ng) return ASTRO_E_SHAPE;
+    const size_t nc = (size_t)g->nx * g->ny * g->nz;
+    k_periodic_yz<<<grid_for(nc, 256), 256, 0, (cudaStream_t)stream>>>(pr, g->nv, g->nx, g->ny,
+                                                                      g->nz, ng);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_outflow_right_x(double* pr, const AstroGrid* g, int ng, void* stream) {
+    if (!pr || !g || ng < 1 || g->nx < 2 * ng + 1) return ASTRO_E_INVALID;
+    const size_t n = (size_t)g->ny * g->nz * ng;
+    k_outflow_right_x<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(pr, g->nv, g->nx,
+                                                                         g->ny, g->nz, ng);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_nozzle_left_x(double* pr, const AstroGrid* g, const AstroNozzle* nz,
+                        const double* draws, const int32_t* rank_map, int32_t n_weighted,
+                        void* stream) {
+    if (!pr || !g || !nz || nz->ng < 1) return ASTRO_E_INVALID;
+    if (nz->perturb && (!draws || !rank_map) && n_weighted > 0) return ASTRO_E_INVALID;
+    if (g->ny - 2 * nz->ng < 1 || g->nz - 2 * nz->ng < 1 || g->nx < nz->ng) return ASTRO_E_SHAPE;
+    if (g->nv < 5 || (nz->physics == 1 && g->nv < 9)) return ASTRO_E_SHAPE;
+    if (nz->n_tracers > 8) return ASTRO_E_UNSUPPORTED;
+    if (nz->n_tracers > 0 && (nz->tracer_offset < 0 || nz->tracer_offset + nz->n_tracers > g->nv))
+        return ASTRO_E_SHAPE;
+    if (nz->two_temperature && nz->thermo_offset < 0) return ASTRO_E_SHAPE;
+    const size_t n = (size_t)nz->ng * (g->ny - 2 * nz->ng) * (g->nz - 2 * nz->ng);
+    k_nozzle<<<grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(pr, g->nv, g->nx, g->ny, g->nz,
+                                                                *nz, draws, rank_map, n_weighted);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_p2c(const AstroParams* p, const double* prim, double* cons, int64_t count, void* stream) {
+    if (!p || !prim || !cons || count < 0) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;
+    k_p2c<<<grid_for(count, 128), 128, 0, (cudaStream_t)stream>>>(*p, prim, cons, count);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t count,
+              AstroC2PStats* stats, void* stream) {
+    if (!p || !prim || !cons || count < 0) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;
+    k_c2p<<<grid_for(count, 128), 128, 0, (cudaStream_t)stream>>>(*p, cons, prim, count, stats);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_cooling_heating(double* pr, const AstroGrid* g, int ng, double dt, double cool,
+                          double heat, double p_max, void* stream) {
+    if (!pr || !g || ng < 0 || g->nv < 5) return ASTRO_E_INVALID;
+    if (cool == 0.0 && heat == 0.0) return ASTRO_OK;
+    if (g->nx <= 2 * ng || g->ny <= 2 * ng || g->nz <= 2 * ng) return ASTRO_OK;
+    const size_t n = (size_t)(g->nx - 2 * ng) * (g->ny - 2 * ng) * (g->nz - 2 * ng);
+    k_cooling<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(pr, g->nx, g->ny, g->nz, ng, dt,
+                                                                 cool, heat, p_max);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, double tau,
+                          int thermo_offset, void* stream) {
+    if (!pr || !g || ng < 0 || thermo_offset < 0) return ASTRO_E_INVALID;
+    if (g->nv < thermo_offset + 2 || tau <= 0.0) return ASTRO_OK;
+    if (g->nx <= 2 * ng || g->ny <= 2 * ng || g->nz <= 2 * ng) return ASTRO_OK;
+    const size_t n = (size_t)(g->nx - 2 * ng) * (g->ny - 2 * ng) * (g->nz - 2 * ng);
+    k_two_temperature<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
+        pr, g->nx, g->ny, g->nz, ng, dt, tau, thermo_offset);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+}  // extern "C"

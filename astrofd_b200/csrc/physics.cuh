@@ -1,0 +1,668 @@
+// physics.cuh -- pointwise SRHD / RMHD physics of AstroFD's right-hand side,
+// as device functions templated on the arithmetic type R (double for the
+// FP64 path, float for the mixed-precision reconstruction/Riemann path).
+//
+// Formulas, clamps and evaluation order follow the reference (paths relative
+// to the AstroFD checkout):
+//   core/srhd_core.py  prim_to_cons :47, cons_to_prim :62, sound_speed :134,
+//                      eig_speeds :143, flux_* :157, hlle :172, hllc_flux_* :189,
+//                      minmod/mc_lim :306,314, ppm_reconstruct :328,
+//                      weno5_left/right :344,362, floor_prim :380
+//   core/rmhd_core.py  limiter :61, floor_prim_rmhd :126, prim_to_cons_rmhd :138,
+//                      _cons_to_prim_hydro :171, rmhd_f_of_Z :229,
+//                      cons_to_prim_rmhd :249, flux_rmhd_* :344, rmhd_fast_speed :420,
+//                      hllc_hydro_flux_* :474, riemann_flux_rmhd_* :570,
+//                      hllc_contact_speed_* :581, hll_d_flux_dir :602
+// Directions are a runtime index n (0 = x, 1 = y, 2 = z); the per-direction
+// copies of the reference differ only in which component is normal.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include "../../include/astrofd.h"
+
+#define AHD __host__ __device__ __forceinline__
+
+namespace astro {
+
+template <typename R> struct C {
+    static constexpr R small = R(1e-12);
+};
+
+template <typename R> AHD R rmax(R a, R b) { return a > b ? a : b; }
+template <typename R> AHD R rmin(R a, R b) { return a < b ? a : b; }
+template <typename R> AHD R rsqrt_(R x) { return sqrt(x); }
+template <typename R> AHD R rabs(R x) { return x < R(0) ? -x : x; }
+
+// Physical parameters in the arithmetic type of the caller.
+template <typename R> struct Phys {
+    R gamma, srhd_gamma, p_max, v_max, glm_ch, glm_cp;
+    int limiter, riemann;
+    AHD static Phys from(const AstroParams& p) {
+        Phys q;
+        q.gamma = R(p.gamma); q.srhd_gamma = R(p.srhd_gamma);
+        q.p_max = R(p.p_max); q.v_max = R(p.v_max);
+        q.glm_ch = R(p.glm_ch); q.glm_cp = R(p.glm_cp);
+        q.limiter = p.limiter; q.riemann = p.riemann;
+        return q;
+    }
+};
+
+// ---------------------------------------------------------------- recon ---
+template <typename R> AHD R minmod(R a, R b) {
+    if (a * b <= R(0)) return R(0);
+    return rabs(a) < rabs(b) ? a : b;
+}
+
+template <typename R> AHD R limiter(int id, R dqL, R dqR) {
+    if (id == ASTRO_LIM_MINMOD) return minmod(dqL, dqR);
+    if (id == ASTRO_LIM_VANLEER) {
+        if (dqL * dqR <= R(0)) return R(0);
+        R denom = dqL + dqR;
+        if (denom == R(0)) return R(0);
+        return (R(2) * dqL * dqR) / denom;
+    }
+    R mm = minmod(dqL, dqR);
+    return minmod(R(0.5) * (dqL + dqR), R(2) * mm);
+}
+
+template <typename R> AHD void ppm(R q_im2, R q_im1, R q_i, R q_ip1, R q_ip2, R& oL, R& oR) {
+    R qL = R(7.0 / 12.0) * (q_im1 + q_i) - R(1.0 / 12.0) * (q_im2 + q_ip1);
+    R qR = R(7.0 / 12.0) * (q_i + q_ip1) - R(1.0 / 12.0) * (q_im1 + q_ip2);
+    R qmax = rmax(rmax(q_im1, q_i), q_ip1);
+    R qmin = rmin(rmin(q_im1, q_i), q_ip1);
+    if (qL > qmax) qL = qmax;
+    if (qL < qmin) qL = qmin;
+    if (qR > qmax) qR = qmax;
+    if (qR < qmin) qR = qmin;
+    if ((qR - q_i) * (q_i - qL) <= R(0)) { qL = q_i; qR = q_i; }
+    oL = qL; oR = qR;
+}
+
+// Jiang-Shu WENO5 value at the face on the (a..e) side; weno5_right of the
+// reference is the same formula with the stencil reversed.
+template <typename R> AHD R weno5(R a, R b, R c, R d, R e) {
+    const R eps = R(1e-12);
+    R t0 = a - R(2) * b + c, u0 = a - R(4) * b + R(3) * c;
+    R t1 = b - R(2) * c + d, u1 = b - d;
+    R t2 = c - R(2) * d + e, u2 = R(3) * c - R(4) * d + e;
+    R IS0 = R(13.0 / 12.0) * (t0 * t0) + R(0.25) * (u0 * u0);
+    R IS1 = R(13.0 / 12.0) * (t1 * t1) + R(0.25) * (u1 * u1);
+    R IS2 = R(13.0 / 12.0) * (t2 * t2) + R(0.25) * (u2 * u2);
+    R a0 = R(0.1) / ((eps + IS0) * (eps + IS0));
+    R a1 = R(0.6) / ((eps + IS1) * (eps + IS1));
+    R a2 = R(0.3) / ((eps + IS2) * (eps + IS2));
+    R s = a0 + a1 + a2;
+    R w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+    R p0 = R(1.0 / 3.0) * a - R(7.0 / 6.0) * b + R(11.0 / 6.0) * c;
+    R p1 = R(-1.0 / 6.0) * b + R(5.0 / 6.0) * c + R(1.0 / 3.0) * d;
+    R p2 = R(1.0 / 3.0) * c + R(5.0 / 6.0) * d - R(1.0 / 6.0) * e;
+    return w0 * p0 + w1 * p1 + w2 * p2;
+}
+
+// Left/right states at the face between cell c-1 and c from a stencil
+// a[0..5] = q(c-3) .. q(c+2).  MUSCL uses a[1..4].
+template <int RECON, typename R> AHD void recon_face(const R* a, int lim, R& qL, R& qR) {
+    if (RECON == ASTRO_RECON_MUSCL) {
+        R slL = limiter(lim, a[2] - a[1], a[3] - a[2]);
+        R slR = limiter(lim, a[3] - a[2], a[4] - a[3]);
+        qL = a[2] + R(0.5) * slL;
+        qR = a[3] - R(0.5) * slR;
+    } else if (RECON == ASTRO_RECON_PPM) {
+        R l0, r0, l1, r1;
+        ppm(a[0], a[1], a[2], a[3], a[4], l0, r0);
+        ppm(a[1], a[2], a[3], a[4], a[5], l1, r1);
+        qL = r0; qR = l1;
+    } else {
+        qL = weno5(a[0], a[1], a[2], a[3], a[4]);
+        qR = weno5(a[5], a[4], a[3], a[2], a[1]);
+    }
+}
+
+template <typename R> AHD R hlle_scalar(R qL, R qR, R fL, R fR, R sL, R sR) {
+    if (sL >= R(0)) return fL;
+    if (sR <= R(0)) return fR;
+    return (sR * fL - sL * fR + sL * sR * (qR - qL)) / (sR - sL + C<R>::small);
+}
+
+template <int N, typename R>
+AHD void hlle(const R* UL, const R* UR, const R* FL, const R* FR, R sL, R sR, R* out) {
+    if (sL >= R(0)) { for (int v = 0; v < N; ++v) out[v] = FL[v]; return; }
+    if (sR <= R(0)) { for (int v = 0; v < N; ++v) out[v] = FR[v]; return; }
+    R inv = sR - sL + C<R>::small;
+#pragma unroll
+    for (int v = 0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) / inv;
+}
+
+template <typename R> AHD void eig_speeds(R vn, R cs, R& lm, R& lp) {
+    R dp = R(1) + vn * cs, dm = R(1) - vn * cs;
+    if (dp == R(0)) dp = C<R>::small;
+    if (dm == R(0)) dm = C<R>::small;
+    R p = (vn + cs) / dp, m = (vn - cs) / dm;
+    if (p > R(1)) p = R(1);
+    if (p < R(-1)) p = R(-1);
+    if (m > R(1)) m = R(1);
+    if (m < R(-1)) m = R(-1);
+    lm = m; lp = p;
+}
+
+// ----------------------------------------------------------------- SRHD ---
+template <typename R> AHD void s_p2c(const Phys<R>& P, const R* q, R* U) {
+    const R gamma = P.srhd_gamma;
+    R rho = q[0], vx = q[1], vy = q[2], vz = q[3], p = q[4];
+    R v2 = vx * vx + vy * vy + vz * vz;
+    if (v2 >= R(1)) v2 = R(1) - R(1e-14);
+    R W = R(1) / rsqrt_(R(1) - v2);
+    R h = R(1) + gamma / (gamma - R(1)) * p / rmax(rho, C<R>::small);
+    R w = rho * h;
+    U[0] = rho * W;
+    R wW2 = w * W * W;
+    U[1] = wW2 * vx;
+    U[2] = wW2 * vy;
+    U[3] = wW2 * vz;
+    U[4] = wW2 - p - U[0];
+}
+
+template <typename R> AHD R s_sound_speed(const Phys<R>& P, R rho, R p) {
+    const R gamma = P.srhd_gamma;
+    R h = R(1) + gamma / (gamma - R(1)) * p / rmax(rho, C<R>::small);
+    R w = rho * h;
+    R cs2 = gamma * p / rmax(w, C<R>::small);
+    if (cs2 < R(0)) cs2 = R(0);
+    if (cs2 > R(1) - R(1e-14)) cs2 = R(1) - R(1e-14);
+    return rsqrt_(cs2);
+}
+
+template <typename R> AHD void floor_prim(const Phys<R>& P, R* q) {
+    if (q[0] < C<R>::small) q[0] = C<R>::small;
+    if (q[4] < C<R>::small) q[4] = C<R>::small;
+    if (q[4] > P.p_max) q[4] = P.p_max;
+    R v2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    R vmax2 = P.v_max * P.v_max;
+    if (v2 >= vmax2) {
+        R fac = P.v_max / rsqrt_(v2 + R(1e-32));
+        q[1] *= fac; q[2] *= fac; q[3] *= fac;
+    }
+}
+
+template <typename R> AHD void s_flux(const Phys<R>& P, int n, const R* q, R* F) {
+    R U[5];
+    s_p2c(P, q, U);
+    R vn = q[1 + n], p = q[4];
+    F[0] = U[0] * vn;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) F[1 + m] = (m == n) ? U[1 + m] * vn + p : U[1 + m] * vn;
+    F[4] = (U[4] + p) * vn;
+}
+
+template <typename R> AHD R contact_speed(int n, const R* UL, const R* UR, R sL, R sR, R pL,
+                                          R pR, R vL, R vR) {
+    R denom = (UL[0] * (sL - vL) - UR[0] * (sR - vR)) + C<R>::small;
+    return (pR - pL + UL[1 + n] * (sL - vL) - UR[1 + n] * (sR - vR)) / denom;
+}
+
+// HLLC for SRHD / the hydro block of RMHD "hlld"
+template <typename R>
+AHD void hllc5(int n, const R* UL, const R* UR, const R* FL, const R* FR, R sL, R sR, R pL,
+               R pR, R vL, R vR, R* out) {
+    if (sL >= R(0)) { for (int v = 0; v < 5; ++v) out[v] = FL[v]; return; }
+    if (sR <= R(0)) { for (int v = 0; v < 5; ++v) out[v] = FR[v]; return; }
+    R DL = UL[0], DR = UR[0];
+    R denom = (DL * (sL - vL) - DR * (sR - vR)) + C<R>::small;
+    R sM = (pR - pL + UL[1 + n] * (sL - vL) - UR[1 + n] * (sR - vR)) / denom;
+    R pStar = R(0.5) * (pL + pR + DL * (sL - vL) * (sM - vL) + DR * (sR - vR) * (sM - vR));
+    const bool left = sM >= R(0);
+    const R* U = left ? UL : UR;
+    const R* F = left ? FL : FR;
+    R s = left ? sL : sR, pK = left ? pL : pR, vK = left ? vL : vR;
+    R den = s - sM + C<R>::small;
+    R fac = (s - vK) / den;
+    R Ust[5];
+    Ust[0] = U[0] * fac;
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+        Ust[1 + m] = (m == n) ? U[1 + m] * fac + (pStar - pK) / den : U[1 + m] * fac;
+    Ust[4] = U[4] * fac + (pStar * sM - pK * vK) / den;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) out[v] = F[v] + s * (Ust[v] - U[v]);
+}
+
+// one SRHD face: floor, p2c, flux, speeds, Riemann (srhd_core.py:517-532)
+template <int RIEMANN, typename R>
+AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
+    R UL[5], UR[5], FL[5], FR[5], lmL, lpL, lmR, lpR;
+    floor_prim(P, qL);
+    floor_prim(P, qR);
+    s_p2c(P, qL, UL);
+    s_p2c(P, qR, UR);
+    s_flux(P, n, qL, FL);
+    s_flux(P, n, qR, FR);
+    R csL = s_sound_speed(P, qL[0], qL[4]), csR = s_sound_speed(P, qR[0], qR[4]);
+    eig_speeds(qL[1 + n], csL, lmL, lpL);
+    eig_speeds(qR[1 + n], csR, lmR, lpR);
+    sL = rmin(lmL, lmR);
+    sR = rmax(lpL, lpR);
+    if (RIEMANN == ASTRO_RIEMANN_HLLC)
+        hllc5(n, UL, UR, FL, FR, sL, sR, qL[4], qR[4], qL[1 + n], qR[1 + n], F);
+    else
+        hlle<5>(UL, UR, FL, FR, sL, sR, F);
+}
+
+// ----------------------------------------------------------------- RMHD ---
+template <typename R> AHD void r_p2c(const Phys<R>& P, const R* qin, R* U) {
+    const R gamma = P.gamma;
+    R rho = qin[0], vx = qin[1], vy = qin[2], vz = qin[3], p = qin[4];
+    R Bx = qin[5], By = qin[6], Bz = qin[7];
+    R v2 = vx * vx + vy * vy + vz * vz;
+    R vmax2 = P.v_max * P.v_max;
+    if (v2 >= vmax2) {
+        R fac = P.v_max / rsqrt_(v2 + R(1e-32));
+        vx *= fac; vy *= fac; vz *= fac;
+    }
+    if (p < C<R>::small) p = C<R>::small;
+    if (p > P.p_max) p = P.p_max;
+    R B2 = Bx * Bx + By * By + Bz * Bz;
+    R W = R(1) / rsqrt_(R(1) - (vx * vx + vy * vy + vz * vz));
+    R h = R(1) + gamma / (gamma - R(1)) * p / rmax(rho, C<R>::small);
+    R rhoh = rho * h;
+    R vb = vx * Bx + vy * By + vz * Bz;
+    R b0 = W * vb;
+    R iW = W;  // divisions kept as in the reference
+    R bx = (Bx + b0 * vx) / iW, by = (By + b0 * vy) / iW, bz = (Bz + b0 * vz) / iW;
+    R b2 = (bx * bx + by * by + bz * bz) - b0 * b0;
+    R rhohW2 = rhoh * W * W;
+    R wtot = rhohW2 + B2;
+    R D = rho * W;
+    U[0] = D;
+    U[1] = wtot * vx - (Bx * vb);
+    U[2] = wtot * vy - (By * vb);
+    U[3] = wtot * vz - (Bz * vb);
+    U[4] = rhohW2 - p + R(0.5) * B2 + R(0.5) * b2 - D;
+    U[5] = Bx; U[6] = By; U[7] = Bz; U[8] = qin[8];
+}
+
+template <typename R> AHD void r_flux(const Phys<R>& P, int n, const R* q, R* F) {
+    R U[9];
+    r_p2c(P, q, U);
+    R v[3] = {q[1], q[2], q[3]}, B[3] = {q[5], q[6], q[7]};
+    R p = q[4], psi = q[8];
+    R B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+    R pt = p + R(0.5) * B2;
+    R vn = v[n], Bn = B[n];
+    F[0] = U[0] * vn;
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+        F[1 + m] = (m == n) ? U[1 + m] * vn + pt - Bn * Bn : U[1 + m] * vn - Bn * B[m];
+    F[4] = (U[4] + pt) * vn - (Bn * (B[0] * v[0] + B[1] * v[1] + B[2] * v[2]));
+#pragma unroll
+    for (int m = 0; m < 3; ++m) F[5 + m] = (m == n) ? psi : v[m] * Bn - vn * B[m];
+    F[8] = P.glm_ch * P.glm_ch * Bn;
+}
+
+template <typename R> AHD R r_fast_speed(const Phys<R>& P, const R* q) {
+    const R G = P.gamma;
+    R rho = q[0], vx = q[1], vy = q[2], vz = q[3], p = q[4];
+    R Bx = q[5], By = q[6], Bz = q[7];
+    R v2 = vx * vx + vy * vy + vz * vz;
+    if (v2 >= P.v_max * P.v_max) v2 = P.v_max * P.v_max - R(1e-14);
+    R W = R(1) / rsqrt_(R(1) - v2);
+    if (rho < C<R>::small) rho = C<R>::small;
+    if (p < C<R>::small) p = C<R>::small;
+    if (p > P.p_max) p = P.p_max;
+    R h = R(1) + G / (G - R(1)) * p / rmax(rho, C<R>::small);
+    R rhoh = rho * h;
+    R vb = vx * Bx + vy * By + vz * Bz;
+    R b0 = W * vb;
+    R bx = (Bx + b0 * vx) / W, by = (By + b0 * vy) / W, bz = (Bz + b0 * vz) / W;
+    R b2 = (bx * bx + by * by + bz * bz) - b0 * b0;
+    R cs2 = G * p / rmax(rhoh, C<R>::small);
+    if (cs2 < R(0)) cs2 = R(0);
+    if (cs2 > R(1) - R(1e-14)) cs2 = R(1) - R(1e-14);
+    R ca2 = b2 / rmax(rhoh + b2, C<R>::small);
+    if (ca2 < R(0)) ca2 = R(0);
+    if (ca2 > R(1) - R(1e-14)) ca2 = R(1) - R(1e-14);
+    R a = cs2 + ca2 - cs2 * ca2;
+    R disc = a * a - R(4) * cs2 * ca2;
+    if (disc < R(0)) disc = R(0);
+    R cf2 = R(0.5) * (a + rsqrt_(disc));
+    if (cf2 < R(0)) cf2 = R(0);
+    if (cf2 > R(1) - R(1e-14)) cf2 = R(1) - R(1e-14);
+    return rsqrt_(cf2);
+}
+
+// hll_d_flux_dir (rmhd_core.py:602-724): approximate HLLD, HLLE on degenerate states
+template <typename R>
+AHD void r_hlld_full(const Phys<R>& P, int n, const R* UL, const R* UR, const R* FL,
+                     const R* FR, R sL, R sR, R pL, R pR, R vL, R vR, R* out) {
+    if (sL >= R(0)) { for (int v = 0; v < 9; ++v) out[v] = FL[v]; return; }
+    if (sR <= R(0)) { for (int v = 0; v < 9; ++v) out[v] = FR[v]; return; }
+    const R SM = C<R>::small;
+    const int t1 = (n == 0) ? 1 : 0, t2 = (n == 2) ? 1 : 2;
+    if (UL[0] <= SM || UR[0] <= SM) { hlle<9>(UL, UR, FL, FR, sL, sR, out); return; }
+    R Bn = R(0.5) * (UL[5 + n] + UR[5 + n]);
+    if (rabs(Bn) < R(1e-8)) { hlle<9>(UL, UR, FL, FR, sL, sR, out); return; }
+    R Bt1L = UL[5 + t1], Bt2L = UL[5 + t2], Bt1R = UR[5 + t1], Bt2R = UR[5 + t2];
+    R sM = contact_speed(n, UL, UR, sL, sR, pL, pR, vL, vR);
+    R DL = UL[0], DR = UR[0];
+    R dLs = sL - sM + SM, dRs = sR - sM + SM;
+    R DstarL = DL * (sL - vL) / dLs;
+    R DstarR = DR * (sR - vR) / dRs;
+    if (DstarL <= SM || DstarR <= SM) { hlle<9>(UL, UR, FL, FR, sL, sR, out); return; }
+    R Bt1Ls = Bt1L * (sL - vL) / dLs, Bt2Ls = Bt2L * (sL - vL) / dLs;
+    R Bt1Rs = Bt1R * (sR - vR) / dRs, Bt2Rs = Bt2R * (sR - vR) / dRs;
+    R denomL = DL * (sL - vL) - Bn * Bn;
+    R denomR = DR * (sR - vR) - Bn * Bn;
+    if (rabs(denomL) < SM || rabs(denomR) < SM) { hlle<9>(UL, UR, FL, FR, sL, sR, out); return; }
+    R vt1L = UL[1 + t1] / rmax(DL, SM), vt2L = UL[1 + t2] / rmax(DL, SM);
+    R vt1R = UR[1 + t1] / rmax(DR, SM), vt2R = UR[1 + t2] / rmax(DR, SM);
+    R vt1Ls = vt1L - Bn * (Bt1L - Bt1Ls) / denomL;
+    R vt2Ls = vt2L - Bn * (Bt2L - Bt2Ls) / denomL;
+    R vt1Rs = vt1R - Bn * (Bt1R - Bt1Rs) / denomR;
+    R vt2Rs = vt2R - Bn * (Bt2R - Bt2Rs) / denomR;
+    R sLs = sM - rabs(Bn) / rsqrt_(DstarL + SM);
+    R sRs = sM + rabs(Bn) / rsqrt_(DstarR + SM);
+    R sqL = rsqrt_(DstarL), sqR = rsqrt_(DstarR);
+    R sgn = (Bn >= R(0)) ? R(1) : R(-1);
+    R den = sqL + sqR + SM;
+    // which fan region: only the needed star states are built
+    int region;
+    if (sL <= R(0) && R(0) <= sLs) region = 0;
+    else if (sLs <= R(0) && R(0) <= sM) region = 1;
+    else if (sM <= R(0) && R(0) <= sRs) region = 2;
+    else if (sRs <= R(0) && R(0) <= sR) region = 3;
+    else { hlle<9>(UL, UR, FL, FR, sL, sR, out); return; }
+    const bool leftside = region <= 1;
+    const R* UK = leftside ? UL : UR;
+    const R* FK = leftside ? FL : FR;
+    R sK = leftside ? sL : sR;
+    R DK = leftside ? DstarL : DstarR;
+    R q[9], UKs[9];
+    // star state on the chosen side (build_state, rmhd_core.py:671-693)
+    q[0] = rmax(DK, SM);
+    q[1 + n] = sM;
+    q[1 + t1] = leftside ? vt1Ls : vt1Rs;
+    q[1 + t2] = leftside ? vt2Ls : vt2Rs;
+    q[4] = (DK == DstarL) ? pL : pR;
+    q[5 + n] = Bn;
+    q[5 + t1] = leftside ? Bt1Ls : Bt1Rs;
+    q[5 + t2] = leftside ? Bt2Ls : Bt2Rs;
+    q[8] = UK[8];
+    r_p2c(P, q, UKs);
+    if (region == 0 || region == 3) {
+#pragma unroll
+        for (int v = 0; v < 9; ++v) out[v] = FK[v] + sK * (UKs[v] - UK[v]);
+        return;
+    }
+    R Dss = R(0.5) * (DstarL + DstarR);
+    R qs[9], Us[9];
+    qs[0] = rmax(Dss, SM);
+    qs[1 + n] = sM;
+    qs[1 + t1] = (sqL * vt1Ls + sqR * vt1Rs + sgn * (Bt1Rs - Bt1Ls)) / den;
+    qs[1 + t2] = (sqL * vt2Ls + sqR * vt2Rs + sgn * (Bt2Rs - Bt2Ls)) / den;
+    qs[4] = (Dss == DstarL) ? pL : pR;
+    qs[5 + n] = Bn;
+    qs[5 + t1] = (sqL * Bt1Rs + sqR * Bt1Ls + sgn * sqL * sqR * (vt1Ls - vt1Rs)) / den;
+    qs[5 + t2] = (sqL * Bt2Rs + sqR * Bt2Ls + sgn * sqL * sqR * (vt2Ls - vt2Rs)) / den;
+    qs[8] = R(0.5) * (UL[8] + UR[8]);
+    r_p2c(P, qs, Us);
+    R sKs = leftside ? sLs : sRs;
+#pragma unroll
+    for (int v = 0; v < 9; ++v) out[v] = FK[v] + sK * (UKs[v] - UK[v]) + sKs * (Us[v] - UKs[v]);
+}
+
+// Riemann dispatch with given speeds; MUSCL_OVR adds the MUSCL-only upwind
+// override of the induction/GLM fluxes for "hlld" (rmhd_core.py:811-831).
+template <int RIEMANN, bool MUSCL_OVR, typename R>
+AHD void r_riemann(const Phys<R>& P, int n, const R* qL, const R* qR, const R* UL,
+                   const R* UR, const R* FL, const R* FR, R sL, R sR, R* out) {
+    R pL = qL[4], pR = qR[4], vL = qL[1 + n], vR = qR[1 + n];
+    if (RIEMANN == ASTRO_RIEMANN_HLLD_FULL) {
+        r_hlld_full(P, n, UL, UR, FL, FR, sL, sR, pL, pR, vL, vR, out);
+    } else if (RIEMANN == ASTRO_RIEMANN_HLLD) {
+        hlle<9>(UL, UR, FL, FR, sL, sR, out);
+        R h5[5];
+        hllc5(n, UL, UR, FL, FR, sL, sR, pL, pR, vL, vR, h5);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) out[v] = h5[v];
+        if (MUSCL_OVR) {
+            R sM = contact_speed(n, UL, UR, sL, sR, pL, pR, vL, vR);
+            const R* Fm = (sM >= R(0)) ? FL : FR;
+#pragma unroll
+            for (int v = 5; v < 9; ++v) out[v] = Fm[v];
+        }
+    } else {
+        hlle<9>(UL, UR, FL, FR, sL, sR, out);
+    }
+}
+
+template <typename R>
+AHD void r_speeds(const Phys<R>& P, int n, const R* qL, const R* qR, R& sL, R& sR) {
+    R lmL, lpL, lmR, lpR;
+    R cfL = r_fast_speed(P, qL), cfR = r_fast_speed(P, qR);
+    eig_speeds(qL[1 + n], cfL, lmL, lpL);
+    eig_speeds(qR[1 + n], cfR, lmR, lpR);
+    sL = rmin(lmL, lmR);
+    sR = rmax(lpL, lpR);
+}
+
+// one RMHD face.  GIVEN: use the supplied (sL, sR) instead of the face's own
+// speeds (the reference's loop-carried x-face speeds, rmhd_core.py:1445,1468).
+template <int RIEMANN, bool MUSCL_OVR, bool GIVEN, typename R>
+AHD void r_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
+    R UL[9], UR[9], FL[9], FR[9];
+    floor_prim(P, qL);
+    floor_prim(P, qR);
+    r_p2c(P, qL, UL);
+    r_p2c(P, qR, UR);
+    r_flux(P, n, qL, FL);
+    r_flux(P, n, qR, FR);
+    if (!GIVEN) r_speeds(P, n, qL, qR, sL, sR);
+    r_riemann<RIEMANN, MUSCL_OVR>(P, n, qL, qR, UL, UR, FL, FR, sL, sR, F);
+}
+
+// ------------------------------------------------------- con2prim (FP64) ---
+struct C2PCount {
+    unsigned newton = 0, bisect = 0, hydro_fallback = 0;
+};
+
+AHD void s_c2p(const Phys<double>& P, const double* U, double* q) {
+    const double gamma = P.srhd_gamma, SM = 1e-12;
+    double D = U[0], Sx = U[1], Sy = U[2], Sz = U[3], tau = U[4];
+    double E = tau + D;
+    double S2 = Sx * Sx + Sy * Sy + Sz * Sz;
+    double p = (gamma - 1.0) * (E - D);
+    if (p < SM) p = SM;
+    if (p > P.p_max) p = P.p_max;
+    bool ok = false;
+    const double vmax2 = P.v_max * P.v_max;
+    for (int it = 0; it < 60; ++it) {
+        double Wm = E + p;
+        double v2 = S2 / (Wm * Wm + SM);
+        if (v2 >= vmax2) v2 = vmax2 - 1e-14;
+        double W = 1.0 / sqrt(1.0 - v2);
+        double rho = D / rmax(W, SM);
+        double h = 1.0 + gamma / (gamma - 1.0) * p / rmax(rho, SM);
+        double f = Wm - rho * h * W * W;
+        double dp = -f;
+        if (dp > 0.5 * p) dp = 0.5 * p;
+        if (dp < -0.5 * p) dp = -0.5 * p;
+        double pn = p + dp;
+        if (pn < SM) pn = SM;
+        if (pn > P.p_max) pn = P.p_max;
+        if (fabs(dp) < 1e-12 * rmax(1.0, pn)) { p = pn; ok = true; break; }
+        p = pn;
+    }
+    if (!ok) {
+        p = (gamma - 1.0) * (E - D);
+        if (p < SM) p = SM;
+        if (p > P.p_max) p = P.p_max;
+    }
+    double Wm = E + p;
+    double vx = Sx / rmax(Wm, SM), vy = Sy / rmax(Wm, SM), vz = Sz / rmax(Wm, SM);
+    double v2 = vx * vx + vy * vy + vz * vz;
+    if (v2 >= vmax2) {
+        double fac = P.v_max / sqrt(v2 + 1e-32);
+        vx *= fac; vy *= fac; vz *= fac;
+    }
+    v2 = vx * vx + vy * vy + vz * vz;
+    if (v2 >= 1.0) v2 = 1.0 - 1e-14;
+    double W = 1.0 / sqrt(1.0 - v2);
+    double rho = D / rmax(W, SM);
+    if (rho < SM) rho = SM;
+    if (p < SM) p = SM;
+    if (p > P.p_max) p = P.p_max;
+    q[0] = rho; q[1] = vx; q[2] = vy; q[3] = vz; q[4] = p;
+}
+
+// _cons_to_prim_hydro (rmhd_core.py:171): the hydro fixed point on p
+AHD void r_c2p_hydro(const Phys<double>& P, double D, double Sx, double Sy, double Sz,
+                     double tau, double* q) {
+    Phys<double> Q = P;
+    Q.srhd_gamma = P.gamma;
+    double U[5] = {D, Sx, Sy, Sz, tau};
+    s_c2p(Q, U, q);
+}
+
+AHD double r_f_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
+                    double SB, double S2) {
+    const double G = P.gamma, SM = 1e-12;
+    double denomZ = rmax(Z, SM);
+    double vb = SB / denomZ;
+    double ZpB = Z + B2;
+    double v2 = (S2 + (SB * SB) * (2.0 * Z + B2) / (denomZ * denomZ)) / (ZpB * ZpB + SM);
+    double vmax2 = P.v_max * P.v_max;
+    if (v2 >= vmax2) v2 = vmax2 - 1e-14;
+    double W2 = 1.0 / (1.0 - v2);
+    double W = sqrt(W2);
+    double rho = D / rmax(W, SM);
+    double h = Z / rmax(rho * W2, SM);
+    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    if (p < SM) p = SM;
+    if (p > P.p_max) p = P.p_max;
+    double b2 = B2 / W2 + vb * vb;
+    double tau_calc = Z - p + 0.5 * B2 + 0.5 * b2 - D;
+    return tau_calc - tau;
+}
+
+// The reference's Newton on Z from a starting value: up to 50 steps with the
+// forward-difference derivative and +-Z/2 step clamp (rmhd_core.py:268-292).
+// Returns true when |f| < 1e-10 max(1, tau).
+AHD bool r_newton(const Phys<double>& P, double& Z, int max_it, double D, double tau,
+                  double B2, double SB, double S2, int* steps = nullptr) {
+    const double tol = 1e-10 * rmax(1.0, tau);
+    for (int it = 0; it < max_it; ++it) {
+        double f = r_f_of_Z(P, Z, D, tau, B2, SB, S2);
+        if (fabs(f) < tol) {
+            if (steps) *steps = it;
+            return true;
+        }
+        double eps = 1e-6 * rmax(1.0, Z);
+        double fp = r_f_of_Z(P, Z + eps, D, tau, B2, SB, S2);
+        double dfdZ = (fp - f) / eps;
+        if (dfdZ == 0.0) break;
+        double dZ = -f / dfdZ;
+        if (dZ > 0.5 * Z) dZ = 0.5 * Z;
+        if (dZ < -0.5 * Z) dZ = -0.5 * Z;
+        Z += dZ;
+        if (Z < 1e-12) Z = 1e-12;
+    }
+    if (steps) *steps = max_it;
+    return false;
+}
+
+// Primitive recovery once Z is known (rmhd_core.py:320-341)
+AHD void r_prims_from_Z(const Phys<double>& P, double Z, const double* U, const double* q0,
+                        double* q, C2PCount& cnt) {
+    const double G = P.gamma, SM = 1e-12;
+    double Sx = U[1], Sy = U[2], Sz = U[3], D = U[0];
+    double Bx = U[5], By = U[6], Bz = U[7];
+    double B2 = Bx * Bx + By * By + Bz * Bz;
+    double SB = Sx * Bx + Sy * By + Sz * Bz;
+    double ZpB = Z + B2;
+    double vb = SB / rmax(Z, SM);
+    double vx = (Sx + vb * Bx) / rmax(ZpB, SM);
+    double vy = (Sy + vb * By) / rmax(ZpB, SM);
+    double vz = (Sz + vb * Bz) / rmax(ZpB, SM);
+    double v2 = vx * vx + vy * vy + vz * vz;
+    double vmax2 = P.v_max * P.v_max;
+    if (v2 >= vmax2) {
+        double fac = P.v_max / sqrt(v2 + 1e-32);
+        vx *= fac; vy *= fac; vz *= fac;
+    }
+    double W = 1.0 / sqrt(1.0 - (vx * vx + vy * vy + vz * vz));
+    double rho = D / rmax(W, SM);
+    double h = Z / rmax(rho * W * W, SM);
+    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    if (!isfinite(rho) || !isfinite(p) || rho <= 0.0 || p <= 0.0) {
+        cnt.hydro_fallback++;
+        rho = q0[0]; vx = q0[1]; vy = q0[2]; vz = q0[3]; p = q0[4];
+    }
+    q[0] = rho; q[1] = vx; q[2] = vy; q[3] = vz; q[4] = p;
+    q[5] = Bx; q[6] = By; q[7] = Bz; q[8] = U[8];
+    floor_prim(P, q);
+}
+
+// Bisection fallback (rmhd_core.py:294-318); Z holds the last Newton iterate
+AHD void r_bisect(const Phys<double>& P, double& Z, double Z1, double D, double tau, double B2,
+                  double SB, double S2) {
+    double Zmin = 1e-12;
+    double Zmax = rmax(rmax(Z, Z1), 1.0);
+    double fmin = r_f_of_Z(P, Zmin, D, tau, B2, SB, S2);
+    double fmax = r_f_of_Z(P, Zmax, D, tau, B2, SB, S2);
+    for (int it = 0; it < 40; ++it) {
+        if (fmin * fmax <= 0.0) break;
+        Zmax *= 2.0;
+        fmax = r_f_of_Z(P, Zmax, D, tau, B2, SB, S2);
+    }
+    if (fmin * fmax <= 0.0) {
+        const double tol = 1e-10 * rmax(1.0, tau);
+        for (int it = 0; it < 60; ++it) {
+            double Zmid = 0.5 * (Zmin + Zmax);
+            double fmid = r_f_of_Z(P, Zmid, D, tau, B2, SB, S2);
+            if (fabs(fmid) < tol) { Z = Zmid; break; }
+            if (fmin * fmid <= 0.0) { Zmax = Zmid; fmax = fmid; }
+            else { Zmin = Zmid; fmin = fmid; }
+            Z = 0.5 * (Zmin + Zmax);
+        }
+    }
+}
+
+// Hydro initial guess and the two Newton starting points Z0, Z1
+AHD void r_c2p_start(const Phys<double>& P, const double* U, double* q0, double& Z0,
+                     double& Z1) {
+    const double G = P.gamma, SM = 1e-12;
+    double D = U[0], tau = U[4];
+    double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+    double tau_h = tau - 0.5 * B2;
+    if (tau_h < SM) tau_h = SM;
+    r_c2p_hydro(P, D, U[1], U[2], U[3], tau_h, q0);
+    double v20 = q0[1] * q0[1] + q0[2] * q0[2] + q0[3] * q0[3];
+    if (v20 >= P.v_max * P.v_max) v20 = P.v_max * P.v_max - 1e-14;
+    double W0 = 1.0 / sqrt(1.0 - v20);
+    double h0 = 1.0 + G / (G - 1.0) * q0[4] / rmax(q0[0], SM);
+    Z0 = rmax(q0[0] * h0 * W0 * W0, SM);
+    Z1 = rmax(D + tau + B2, SM);
+}
+
+// Full reference con2prim (cons_to_prim_rmhd, rmhd_core.py:249-341)
+AHD void r_c2p(const Phys<double>& P, const double* U, double* q, C2PCount& cnt) {
+    double D = U[0], tau = U[4];
+    double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+    double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
+    double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+    double q0[5], Z0, Z1;
+    r_c2p_start(P, U, q0, Z0, Z1);
+    double Z = Z0;
+    bool ok = r_newton(P, Z, 50, D, tau, B2, SB, S2);
+    if (!ok) {
+        Z = Z1;
+        ok = r_newton(P, Z, 50, D, tau, B2, SB, S2);
+    }
+    if (ok) cnt.newton++;
+    else {
+        cnt.bisect++;
+        r_bisect(P, Z, Z1, D, tau, B2, SB, S2);
+    }
+    r_prims_from_Z(P, Z, U, q0, q, cnt);
+}
+
+}  // namespace astro

@@ -1,0 +1,420 @@
+#!/usr/bin/env python3
+"""Benchmark: zone-updates/s of AstroFD's per-step RHS on the B200.
+
+Workload (default): RMHD 256^3 magnetised jet, Gamma = 4/3, WENO5 + "hlld"
+(HLLC hydro + HLLE field), SSPRK3, resistivity 1e-4, two-temperature
+(TEI_TAU 0.1) and cooling (lambda 0.01), NG = 3, 11 variables.  One "step" is
+one iteration of the reference driver loop (solvers/srhd3d_mpi_muscl.py:276-326):
+ghost fill, SSPRK3 step, ghost fill, cooling, two-temperature.  dt = CFL dx
+with CFL 0.35 (the reference uses amax = 1 for RMHD).
+
+Arms
+  default            mixed precision (float32 reconstruction/Riemann, float64
+                     state / RK / con2prim) on the GPU; also times the plain
+                     float64 GPU path for the speed-up in the same line.
+  --impl reference   the reference algorithm on the host cores (the C port of
+                     the reference's Numba kernels, all threads), on a bounded
+                     x-slab sample of the same state.
+
+Timing: CUDA events on the launching stream around exactly K steps after W
+warm-up steps, barrier + synchronize on both sides, max over ranks.  Every
+array (1.6 GB each) is larger than the 126 MB L2, so no explicit flush.
+With --gpus N each rank advances its own full-size replica (the north-star path
+is single-GPU; there is no data-path collective), value = N x per-rank work /
+max time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s 256^3 RMHD (mixed+learned c2p vs FP64 plain, L1<1e-4)"
+UNIT = "zone-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--flux-mode", default="conservative", choices=["conservative", "reference"])
+    ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-x-cells", type=int, default=4,
+                    help="x-slab thickness of the bounded CPU sample")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ ranks --
+def dist_init(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------- GPU ---
+class DriverStep:
+    """One reference driver-loop iteration on device tensors."""
+
+    def __init__(self, n, ng, core_cfg, nozzle_cfg, src_cfg):
+        from astrofd_b200.core import boundary, nozzle, rmhd_core, source_terms
+        self.B, self.N, self.R, self.S = boundary, nozzle, rmhd_core, source_terms
+        self.n, self.ng = n, ng
+        self.d = 1.0 / n
+        self.dt = core_cfg["CFL"] * self.d
+        self.noz, self.src = nozzle_cfg, src_cfg
+        self.rng = np.random.default_rng(1234)
+
+    def bcs(self, pr):
+        self.B.apply_periodic_yz(pr, self.ng)
+        self.B.apply_outflow_right_x(pr, self.ng)
+        self.N.apply_nozzle_left_x(pr, self.d, self.d, self.d, self.n, self.n, 0.5, 0.5,
+                                   self.rng, self.noz)
+
+    def __call__(self, pr, out, profile=False):
+        d = self.d
+        self.bcs(pr)
+        times = None
+        if profile:
+            _, times, launches = self.R.engine().step_profiled(pr, d, d, d, self.dt, 3, out)
+            times = (times, launches)
+        else:
+            self.R.step_ssprk3(pr, d, d, d, self.dt, out=out)
+        self.bcs(out)
+        self.S.apply_cooling_heating(out, self.dt, self.src)
+        self.S.apply_two_temperature(out, self.dt, self.src)
+        return out, pr, times
+
+
+def time_arm(args, world, prec, pr_host, cfgs, profile):
+    import torch
+    from astrofd_b200 import _lib
+    from astrofd_b200.core import rmhd_core
+    core, noz, src = cfgs
+    cfg = dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode)
+    rmhd_core.configure(cfg)
+    step = DriverStep(args.n, 3, core, noz, src)
+    a = torch.from_numpy(pr_host).to("cuda")
+    b = torch.empty_like(a)
+    for _ in range(args.warmup):
+        a, b, _ = step(a, b)
+    rmhd_core.c2p_stats(reset=True)
+    L = _lib.load()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    prof_ms = np.zeros(4)
+    prof_n = np.zeros(4, dtype=np.int64)
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = L.astro_launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            a, b, t = step(a, b, profile=profile)
+            if t is not None:
+                prof_ms += np.array(t[0])
+                prof_n += np.array(t[1])
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    launches = L.astro_launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    finite = bool(torch.isfinite(a).all().item())
+    stats = rmhd_core.c2p_stats(reset=True)
+    return dict(ms=ms, launches=int(launches), prof_ms=prof_ms, prof_n=prof_n,
+                clocks=clk.summary(), finite=finite, state=a, c2p=stats)
+
+
+def time_e2e(args, world, prec, pr_host, cfgs):
+    """Public API with host buffers: each step uploads the block from pinned
+    host memory and reads the result back."""
+    import torch
+    from astrofd_b200.core import rmhd_core
+    core, noz, src = cfgs
+    rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode))
+    step = DriverStep(args.n, 3, core, noz, src)
+    host_in = torch.from_numpy(pr_host).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    a = torch.empty(host_in.shape, dtype=torch.float64, device="cuda")
+    b = torch.empty_like(a)
+    stream = torch.cuda.current_stream()
+
+    def one():
+        a.copy_(host_in, non_blocking=True)
+        out, _, _ = step(a, b)
+        host_out.copy_(out, non_blocking=True)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        one()
+    k = max(1, min(args.steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(k):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    nbytes = host_in.numel() * 8
+    return dict(ms=ms, steps=k, h2d=nbytes, d2h=nbytes)
+
+
+# ------------------------------------------------------------------- CPU ---
+def cpu_sample(args, steps, warmup):
+    """The reference algorithm (C port of the Numba kernels) on the host cores:
+    the same driver iteration on an x-slab of the same state."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
+    n, ng, xc = args.n, 3, args.cpu_x_cells
+    core, noz, src = rmhd_jet_config(n, ng)
+    # the reference's own arithmetic (loop-carried x-face speeds, its resistive
+    # handling), whatever flux mode the GPU arm runs
+    cfg = dict(core, FLUX_MODE="reference")
+    P = O.params_from_config("rmhd", cfg)
+    pr = rmhd_jet(n, ng, x_cells=xc)
+    d = 1.0 / n
+    dt = core["CFL"] * d
+    rng = np.random.default_rng(1234)
+
+    def bcs(a):
+        O.apply_periodic_yz(a, ng)
+        O.apply_outflow_right_x(a, ng)
+        O.apply_nozzle_left_x(a, d, d, d, n, n, 0.5, 0.5, rng, noz)
+
+    def one(a):
+        bcs(a)
+        a = O.step(P, a, d, d, d, dt, 3)
+        bcs(a)
+        O.apply_cooling_heating(a, dt, src)
+        O.apply_two_temperature(a, dt, src)
+        return a
+
+    for _ in range(warmup):
+        pr = one(pr)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pr = one(pr)
+    sec = time.perf_counter() - t0
+    zones = xc * n * n * steps
+    return dict(value=zones / sec, cores=O.num_threads(), kind="port",
+                sample=f"{steps} driver steps on a {xc}x{n}x{n} x-slab of the {n}^3 state "
+                       f"(C port of the reference's Numba kernels, OpenMP)")
+
+
+# ------------------------------------------------------------------ main ---
+def roofline(args, prof_ms, prof_n, prec):
+    """Dominant kernel class and its achieved HBM bandwidth (algorithmic bytes)."""
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    which = "measured" if "hbm_gbs" in peaks else "fallback"
+    cls = int(np.argmax(prof_ms[:2]))
+    nlaunch = max(int(prof_n[cls]), 1)
+    avg_s = prof_ms[cls] / nlaunch / 1e3
+    n, ng, nv, nm = args.n, 3, 11, 9
+    N = n + 2 * ng
+    rs = 4 if prec == "mixed" else 8
+    if cls == 0:
+        # face pass in one direction: each face reads one new primitive column
+        # (nm float64) and writes its flux (nm values); faces ~ n^3 (+1 plane)
+        units = (n + 1) * n * n
+        per_unit = nm * 8 + nm * rs
+        name = "k_face (reconstruction + Riemann, one direction)"
+    else:
+        # stage update over all N^3 cells: 3 face fluxes, pr0 and pr_k (nv
+        # float64 each), U_k-1 and U_k (nm float64), writes next primitives
+        units = N ** 3
+        per_unit = 3 * nm * rs + 2 * nv * 8 + 2 * nm * 8 + nv * 8
+        name = "k_update (divergence + SSPRK + con2prim)"
+    achieved = units * per_unit / avg_s / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        t = json.load(open(tf)).get(f"{prec}:{cls}")
+        if t:
+            traffic = t
+    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1),
+            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "peak_source": which,
+            "bytes_per_launch": units * per_unit, "avg_launch_ms": round(avg_s * 1e3, 4),
+            "class_share": round(float(prof_ms[cls] / max(prof_ms.sum(), 1e-30)), 3)}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        r = cpu_sample(args, args.steps, args.warmup)
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "impl": "reference", "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"rmhd-jet-{args.n}^3 weno5/hlld ssprk3 + resistive + "
+                                       "two-temperature + cooling", "sample_x_cells":
+                               args.cpu_x_cells, "flux_mode": "reference"},
+                "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"],
+                                 "kind": r["kind"], "sample": r["sample"]},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "vs_baseline": None}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
+    rank, world, local = dist_init(args)
+    n = args.n
+    cfgs = rmhd_jet_config(n, 3)
+    pr_host = rmhd_jet(n, 3, seed=2024 + rank)
+    zones = n ** 3 * args.steps * world
+
+    mixed = time_arm(args, world, "mixed", pr_host, cfgs, profile=True)
+    fp64 = None if args.no_fp64 else time_arm(args, world, "fp64", pr_host, cfgs, profile=False)
+    e2e = None if args.no_e2e else time_e2e(args, world, "mixed", pr_host, cfgs)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample(args, steps=1, warmup=0)
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    value = zones / (mixed["ms"] / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": mixed["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 state/con2prim, f32 flux",
+        "data": "synthetic (seeded magnetised jet)",
+        "config": {"workload": f"rmhd-jet-{n}^3 weno5/hlld ssprk3 + resistive 1e-4 + "
+                               "two-temperature + cooling (driver-loop iteration)",
+                   "grid": [n, n, n], "ng": 3, "nv": 11, "precision": "mixed",
+                   "c2p_guess": "reference", "flux_mode": args.flux_mode,
+                   "l2": "inputs larger than L2 (1.6 GB arrays)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "gpu_launches": mixed["launches"],
+        "clocks": mixed["clocks"],
+        "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed"),
+        "kernel_ms_per_step": {"face": round(mixed["prof_ms"][0] / args.steps, 3),
+                               "update": round(mixed["prof_ms"][1] / args.steps, 3)},
+        "finite": mixed["finite"],
+        "c2p": mixed["c2p"],
+    }
+    if fp64 is not None:
+        v64 = zones / (fp64["ms"] / 1e3)
+        line["fp64_value"] = v64
+        line["speedup_vs_fp64"] = value / v64
+        a, b = mixed["state"], fp64["state"]
+        line["rho_l1_vs_fp64_after_steps"] = float(
+            ((a[0] - b[0]).abs().mean() / b[0].abs().mean()).item())
+    if e2e is not None:
+        line["e2e"] = {"value": n ** 3 * e2e["steps"] * world / (e2e["ms"] / 1e3), "unit": UNIT,
+                       "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"],
+                                "kind": cpu["kind"], "sample": cpu["sample"]}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * astrofd.h -- C ABI of libastrofd_b200.so, the B200 (sm_100a) implementation
+ * of AstroFD's per-step finite-volume right-hand side.
+ *
+ * Conventions
+ *   - Every array pointer is DEVICE memory (CUDA global memory on the device
+ *     that is current for the calling thread) unless a parameter name ends in
+ *     _host.  Primitive blocks are float64, C-contiguous pr[v][i][j][k] with
+ *     extents (nv, nx, ny, nz) INCLUDING ghost cells, k fastest -- the layout
+ *     of the reference's numpy blocks (solvers/srhd3d_mpi_muscl.py:128).
+ *   - `stream` is a cudaStream_t passed as void*; NULL means the legacy
+ *     default stream.  All entry points are stream-ordered and asynchronous
+ *     unless stated otherwise; none synchronises the device.
+ *   - Scratch memory is caller-owned: query its size with the matching
+ *     *_workspace_bytes() call and pass a device buffer of at least that size.
+ *   - Return value: 0 on success, a negative ASTRO_E* code on failure
+ *     (astro_error_string() describes it).  Numerical failures inside kernels
+ *     (con2prim falling back, iteration caps) never trap: they are counted in
+ *     AstroC2PStats.
+ *   - Thread safety: no mutable global state; calls on different streams are
+ *     independent.
+ */
+#ifndef ASTROFD_B200_H
+#define ASTROFD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASTRO_OK 0
+#define ASTRO_E_INVALID (-1)      /* bad argument (null pointer, bad enum)        */
+#define ASTRO_E_SHAPE (-2)        /* grid too small for the stencil / ghosts      */
+#define ASTRO_E_WORKSPACE (-3)    /* workspace missing or smaller than required    */
+#define ASTRO_E_UNSUPPORTED (-4)  /* configuration outside the supported path      */
+#define ASTRO_E_CUDA (-5)         /* a CUDA launch or runtime call failed          */
+
+/* physics */
+#define ASTRO_SRHD 0
+#define ASTRO_RMHD 1
+/* reconstruction */
+#define ASTRO_RECON_MUSCL 0
+#define ASTRO_RECON_PPM 1
+#define ASTRO_RECON_WENO 2
+/* MUSCL limiter */
+#define ASTRO_LIM_MC 0
+#define ASTRO_LIM_MINMOD 1
+#define ASTRO_LIM_VANLEER 2
+/* Riemann solver: SRHD 0 = HLLE, 1 = HLLC; RMHD 0 = HLLE,
+ * 1 = "hlld" (HLLC hydro + HLLE field), 2 = "hlld_full" (approximate HLLD) */
+#define ASTRO_RIEMANN_HLLE 0
+#define ASTRO_RIEMANN_HLLC 1
+#define ASTRO_RIEMANN_HLLD 1
+#define ASTRO_RIEMANN_HLLD_FULL 2
+/* flux_mode */
+#define ASTRO_FLUX_REFERENCE 0    /* reproduce the reference's x-face speeds     */
+#define ASTRO_FLUX_CONSERVATIVE 1 /* every face evaluated once, from both sides  */
+/* precision */
+#define ASTRO_PREC_FP64 0         /* everything in float64                        */
+#define ASTRO_PREC_MIXED 1        /* reconstruction + Riemann in float32; state,
+                                     RK accumulation and con2prim in float64     */
+/* con2prim initial guess */
+#define ASTRO_GUESS_REFERENCE 0   /* hydro fixed point, as the reference          */
+#define ASTRO_GUESS_LEARNED 1     /* MLP guess + <=2 Newton polish, full fallback */
+
+/* Mirrors the keys read by srhd_core.configure (core/srhd_core.py:18-41) and
+ * rmhd_core.configure (core/rmhd_core.py:21-50). */
+typedef struct AstroParams {
+    int32_t physics, recon, limiter, riemann;
+    int32_t n_passive, passive_offset, resistive, flux_mode;
+    int32_t precision, c2p_guess, reserved0, reserved1;
+    double gamma;        /* RMHD adiabatic index (GAMMA)                      */
+    double srhd_gamma;   /* SRHD kernels: the reference freezes this at 5/3   */
+    double p_max, v_max, glm_ch, glm_cp, resistivity;
+} AstroParams;
+
+typedef struct AstroGrid {
+    int32_t nv, nx, ny, nz;   /* extents including ghosts */
+    double dx, dy, dz;
+} AstroGrid;
+
+/* Nozzle inflow on the left x ghost layers (core/nozzle.py:27-91). */
+typedef struct AstroNozzle {
+    int32_t ng, profile;        /* profile 0 top_hat, 1 taper, 2 parabolic          */
+    int32_t perturb, physics;   /* perturb != 0: draws supplied; physics 1 = rmhd   */
+    int32_t b_init;             /* 0 none, 1 poloidal (Bx), 2 toroidal (By = B0 s)  */
+    int32_t n_tracers, tracer_offset, two_temperature, thermo_offset, reserved;
+    double radius, shear_thick, gamma_jet, eta_rho, p_eq, rho_amb;
+    double vx_amb, vy_amb, vz_amb, turb_vamp, turb_pamp, b0, te, ti;
+    double dy, dz, y0, z0;
+    double tracer_nozzle[8], tracer_amb[8];
+} AstroNozzle;
+
+/* con2prim outcome counters accumulated by astro_step/astro_c2p */
+typedef struct AstroC2PStats {
+    unsigned long long cells;          /* con2prim calls                            */
+    unsigned long long newton;         /* converged by Newton (any start)          */
+    unsigned long long bisection;      /* reached the bisection fallback            */
+    unsigned long long hydro_fallback; /* invalid result -> hydro guess kept        */
+    unsigned long long learned_polish; /* learned guess converged within <=2 steps  */
+    unsigned long long learned_fallback; /* learned guess failed -> full solve      */
+    unsigned long long polish_steps;   /* total polish steps taken                  */
+    unsigned long long reserved;
+} AstroC2PStats;
+
+/* --- build / diagnostics ------------------------------------------------ */
+int astro_version(void);
+const char* astro_error_string(int code);
+
+/* --- right-hand side ----------------------------------------------------
+ * Replaces srhd_core.compute_rhs_{muscl,ppm,weno} (core/srhd_core.py:469,927,1167)
+ * and rmhd_core.compute_rhs_{rmhd,ppm,weno} (core/rmhd_core.py:749,1280,1440).
+ * rhs has extents (nm + n_passive, nx, ny, nz), nm = 5 (SRHD) or 9 (RMHD), and is
+ * zero outside the reference's loop bounds. */
+size_t astro_rhs_workspace_bytes(const AstroParams* p, const AstroGrid* g);
+int astro_rhs(const AstroParams* p, const AstroGrid* g, const double* pr, double* rhs,
+              void* work, size_t work_bytes, void* stream);
+
+/* --- one SSPRK step -----------------------------------------------------
+ * Replaces {srhd,rmhd}_core.step_ssprk2/3 (core/srhd_core.py:1286,1334;
+ * core/rmhd_core.py:1559,1609): returns the new primitive block in pr_out
+ * (pr_in is not modified; pr_out must not alias pr_in).  rk_order is 2 or 3.
+ * If stats is non-NULL the step's con2prim counters are added to it (device
+ * memory, one AstroC2PStats). */
+size_t astro_step_workspace_bytes(const AstroParams* p, const AstroGrid* g);
+int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in,
+               double* pr_out, double dt, int rk_order, void* work, size_t work_bytes,
+               AstroC2PStats* stats, void* stream);
+
+/* Per-kernel-class device time of one step, from CUDA events recorded after
+ * every launch.  Classes: 0 face-flux passes, 1 stage update (divergence, RK,
+ * con2prim), 2 other (ghost fills, reductions, sources), 3 reserved. */
+typedef struct AstroKernelTimes {
+    double ms[4];
+    int32_t launches[4];
+} AstroKernelTimes;
+
+/* astro_step with per-launch event timing filled into *times.  Synchronises
+ * the stream before returning (profiling use, e.g. a benchmark's roofline).
+ * No counterpart in the reference (which has no device kernels to time). */
+int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* pr_in,
+                        double* pr_out, double dt, int rk_order, void* work, size_t work_bytes,
+                        AstroC2PStats* stats, void* stream, AstroKernelTimes* times);
+
+/* Number of kernels this library has launched in the process so far
+ * (a diagnostic counter; no counterpart in the reference). */
+unsigned long long astro_launch_count(void);
+
+/* --- CFL speed ----------------------------------------------------------
+ * Replaces srhd_core.max_char_speed (core/srhd_core.py:1268): writes the max
+ * characteristic speed over i,j,k in [1, n-1) to out (device double). */
+size_t astro_max_char_speed_workspace_bytes(void);
+int astro_max_char_speed(const AstroParams* p, const AstroGrid* g, const double* pr,
+                         double* out, void* work, size_t work_bytes, void* stream);
+
+/* --- ghost fills (in place) ----------------------------------------------
+ * Replace boundary.apply_periodic_yz / apply_outflow_right_x
+ * (core/boundary.py:4,10) and nozzle.apply_nozzle_left_x (core/nozzle.py:27).
+ * draws: 3 uniforms per perturbed nozzle cell in the reference's draw order
+ * (g, j, k), or NULL when unperturbed; rank_map: (ny-2ng)*(nz-2ng) int32 giving
+ * each interior (j,k) its rank among cells with nozzle weight > 0 (or -1). */
+int astro_periodic_yz(double* pr, const AstroGrid* g, int ng, void* stream);
+int astro_outflow_right_x(double* pr, const AstroGrid* g, int ng, void* stream);
+int astro_nozzle_left_x(double* pr, const AstroGrid* g, const AstroNozzle* nz,
+                        const double* draws, const int32_t* rank_map, int32_t n_weighted,
+                        void* stream);
+
+/* --- pointwise conversions ----------------------------------------------
+ * Array forms of prim_to_cons / cons_to_prim (core/srhd_core.py:47,62) and
+ * prim_to_cons_rmhd / cons_to_prim_rmhd (core/rmhd_core.py:138,249).
+ * Arrays are (nm, count) float64. */
+int astro_p2c(const AstroParams* p, const double* prim, double* cons, int64_t count,
+              void* stream);
+int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t count,
+              AstroC2PStats* stats, void* stream);
+
+/* --- operator-split post-step sources (core/source_terms.py:5,30) -------- */
+int astro_cooling_heating(double* pr, const AstroGrid* g, int ng, double dt, double cool,
+                          double heat, double p_max, void* stream);
+int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, double tau,
+                          int thermo_offset, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASTROFD_B200_H */

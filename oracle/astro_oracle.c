@@ -52,7 +52,9 @@ typedef struct {
     int n_passive;
     int passive_offset;
     int resistive;
-    int pad_;
+    int flux_mode;      /* 0 = the reference's own arithmetic; 1 = each RMHD
+                           PPM/WENO x face with its own speeds and the
+                           resistive term applied once for every recon      */
     double gamma;       /* RMHD gamma; SRHD kernels always use 5/3 (quirk)  */
     double p_max, v_max, glm_ch, glm_cp, resistivity;
 } OParams;
@@ -828,7 +830,7 @@ static void s_rhs(const OParams* pa, const OGrid* g, const double* pr, double dd
     memset(rhs, 0, sizeof(double) * (size_t)nr * g->nx * g->ny * g->nz);
     int lo = bounds_lo(pa), ho = bounds_hi_off(pa);
     int i1 = g->nx - ho, j1 = g->ny - ho, k1 = g->nz - ho;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for collapse(2) schedule(static)
     for (int i = lo; i < i1; ++i)
         for (int j = lo; j < j1; ++j)
             for (int k = lo; k < k1; ++k) {
@@ -891,13 +893,15 @@ static void r_rhs(const OParams* pa, const OGrid* g, const double* pr, double dd
     int lo = bounds_lo(pa), ho = bounds_hi_off(pa);
     int i1 = g->nx - ho, j1 = g->ny - ho, k1 = g->nz - ho;
     const int muscl = (pa->recon == 0);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for collapse(2) schedule(static)
     for (int i = lo; i < i1; ++i) {
-        /* loop-carried (sL, sR) entering row i: +-1 for the very first cell,
-         * else the z-back face speeds of the previous cell in loop order */
-        double cL = -1.0, cR = 1.0;
-        if (!muscl && i > lo) r_zback_speeds(pa, g, pr, i - 1, j1 - 1, k1 - 1, &cL, &cR);
-        for (int j = lo; j < j1; ++j)
+        for (int j = lo; j < j1; ++j) {
+            /* loop-carried (sL, sR) entering row (i, j): +-1 for the very first
+             * cell, else the z-back face speeds of the previous cell in the
+             * reference's serial i-j-k order */
+            double cL = -1.0, cR = 1.0;
+            if (!muscl && j > lo) r_zback_speeds(pa, g, pr, i, j - 1, k1 - 1, &cL, &cR);
+            else if (!muscl && i > lo) r_zback_speeds(pa, g, pr, i - 1, j1 - 1, k1 - 1, &cL, &cR);
             for (int k = lo; k < k1; ++k) {
                 double r[9] = {0};
                 for (int n = 0; n < 3; ++n) {
@@ -906,7 +910,7 @@ static void r_rhs(const OParams* pa, const OGrid* g, const double* pr, double dd
                     Face fa, fb;
                     face_states(pa, g, pr, 9, n, i, j, k, qL, qR);
                     face_states(pa, g, pr, 9, n, o[0], o[1], o[2], qL2, qR2);
-                    if (!muscl && n == 0) r_face_given(pa, 0, qL, qR, cL, cR, &fa);
+                    if (!muscl && n == 0 && pa->flux_mode == 0) r_face_given(pa, 0, qL, qR, cL, cR, &fa);
                     else r_face(pa, n, muscl, qL, qR, &fa);
                     r_face(pa, n, muscl, qL2, qR2, &fb);
                     if (!muscl && n == 2) { cL = fa.sL; cR = fa.sR; }
@@ -931,6 +935,7 @@ static void r_rhs(const OParams* pa, const OGrid* g, const double* pr, double dd
                 r[8] -= pa->glm_cp * pa->glm_cp * P(8, i, j, k);
                 int nres = (pa->resistive && pa->resistivity > 0.0)
                                ? (pa->recon == 0 ? 1 : (pa->recon == 1 ? 2 : 0)) : 0;
+                if (pa->flux_mode == 1) nres = (pa->resistive && pa->resistivity > 0.0) ? 1 : 0;
                 for (int rep = 0; rep < nres; ++rep) {
                     double ix2 = 1.0 / (dd[0] * dd[0] + SMALL);
                     double iy2 = 1.0 / (dd[1] * dd[1] + SMALL);
@@ -944,6 +949,7 @@ static void r_rhs(const OParams* pa, const OGrid* g, const double* pr, double dd
                 }
                 for (int v = 0; v < 9; ++v) rhs[IX(&gr, v, i, j, k)] = r[v];
             }
+        }
     }
 }
 

@@ -23,7 +23,7 @@ class OParams(C.Structure):
     _fields_ = [("physics", C.c_int), ("recon", C.c_int), ("limiter", C.c_int),
                 ("riemann", C.c_int), ("n_passive", C.c_int),
                 ("passive_offset", C.c_int), ("resistive", C.c_int),
-                ("pad_", C.c_int), ("gamma", C.c_double), ("p_max", C.c_double),
+                ("flux_mode", C.c_int), ("gamma", C.c_double), ("p_max", C.c_double),
                 ("v_max", C.c_double), ("glm_ch", C.c_double),
                 ("glm_cp", C.c_double), ("resistivity", C.c_double)]
 
@@ -111,6 +111,7 @@ def params_from_config(physics, cfg):
     p.glm_ch = float(cfg.get("GLM_CH", 1.0))
     p.glm_cp = float(cfg.get("GLM_CP", 0.1))
     p.resistivity = float(cfg.get("RESISTIVITY", 0.0))
+    p.flux_mode = 1 if str(cfg.get("FLUX_MODE", "reference")).lower() == "conservative" else 0
     return p
 
 

@@ -1,0 +1,71 @@
+"""CPU-side checks of the C ABI: the library loads and exports every entry
+point include/astrofd.h declares, and host-side validation works without a
+GPU (no compute calls here)."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from astrofd_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "astrofd.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(astro_[a-z0-9_]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from astrofd_b200 import build
+    if not os.path.exists(_lib.LIB_PATH):
+        build.build()
+    return _lib.load()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = header_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _lib.PROTOS, f"{n} has no ctypes prototype"
+
+
+def test_struct_sizes_match_header_layout():
+    assert C.sizeof(_lib.AstroParams) == 12 * 4 + 7 * 8
+    assert C.sizeof(_lib.AstroGrid) == 4 * 4 + 3 * 8
+    assert C.sizeof(_lib.AstroC2PStats) == 8 * 8
+    assert C.sizeof(_lib.AstroNozzle) == 10 * 4 + 18 * 8 + 16 * 8
+
+
+def test_error_strings_and_validation(lib):
+    assert lib.astro_version() >= 10000
+    assert lib.astro_error_string(-3) == b"workspace missing or too small"
+    p = _lib.AstroParams()
+    p.physics, p.recon, p.riemann = 1, 2, 2
+    p.gamma = p.srhd_gamma = 4.0 / 3.0
+    g = _lib.AstroGrid(9, 22, 22, 22, 0.1, 0.1, 0.1)
+    nb = lib.astro_step_workspace_bytes(C.byref(p), C.byref(g))
+    assert nb > 9 * 22 ** 3 * 8 * 3
+    # invalid enum -> 0 bytes and an error code, no device work
+    p.riemann = 7
+    assert lib.astro_step_workspace_bytes(C.byref(p), C.byref(g)) == 0
+    assert lib.astro_rhs(C.byref(p), C.byref(g), None, None, None, 0, None) == -1
+    # SRHD blocks carrying dissipation fields are rejected
+    p.physics, p.riemann = 0, 0
+    g.nv = 15
+    assert lib.astro_rhs_workspace_bytes(C.byref(p), C.byref(g)) == 0
+
+
+def test_product_raises_without_gpu_instead_of_falling_back():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    import numpy as np
+    from astrofd_b200.core import srhd_core
+    pr = np.ones((5, 12, 12, 12))
+    with pytest.raises(_lib.AstroError):
+        srhd_core.compute_rhs_muscl(pr, 12, 12, 12, 0.1, 0.1, 0.1)
