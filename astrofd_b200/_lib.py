@@ -74,6 +74,9 @@ PROTOS = {
     "astro_rhs_workspace_bytes": (C.c_size_t, [C.POINTER(AstroParams), C.POINTER(AstroGrid)]),
     "astro_rhs": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP, _DP, _VP,
                             C.c_size_t, _VP]),
+    "astro_rhs_static_max_bytes": (C.c_size_t, []),
+    "astro_rhs_static": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP, _DP,
+                                   _VP]),
     "astro_step_workspace_bytes": (C.c_size_t, [C.POINTER(AstroParams), C.POINTER(AstroGrid)]),
     "astro_step": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP, _DP,
                              C.c_double, C.c_int, _VP, C.c_size_t, _VP, _VP]),

@@ -23,6 +23,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <mutex>
 
 #include "physics.cuh"
 
@@ -742,6 +743,42 @@ int grid_for(size_t n, int block) {
 
 }  // namespace
 
+// ------------------------------------------------- allocation-free rhs ---
+// Scratch for astro_rhs_static: a fixed-size array in the module's device
+// memory.  Every device that loads this library holds it (32 MiB) until the
+// process exits.  Host code must not use the symbol's name as a device
+// pointer: the device address is looked up once per device with
+// cudaGetSymbolAddress (with that device current) and cached here.
+static constexpr size_t kStaticScratchBytes = size_t(32) << 20;
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::atomic<void*> g_static_scratch_addr[kMaxDevices];
+std::mutex g_static_scratch_mu;
+
+// Device address of g_static_scratch on the current device (nullptr on error).
+void* static_scratch_address(int* err) {
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        *err = ASTRO_E_CUDA;
+        return nullptr;
+    }
+    void* a = g_static_scratch_addr[dev].load(std::memory_order_acquire);
+    if (a) return a;
+    std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+    a = g_static_scratch_addr[dev].load(std::memory_order_acquire);
+    if (a) return a;
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) {
+        *err = ASTRO_E_CUDA;
+        return nullptr;
+    }
+    g_static_scratch_addr[dev].store(ptr, std::memory_order_release);
+    return ptr;
+}
+}  // namespace
+
 // =================================================================== C ABI ==
 extern "C" {
 
@@ -939,6 +976,29 @@ int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, dou
         pr, g->nx, g->ny, g->nz, ng, dt, tau, thermo_offset);
     mark(2, (cudaStream_t)stream);
     return cuda_status(cudaGetLastError());
+}
+
+size_t astro_rhs_static_max_bytes(void) { return kStaticScratchBytes; }
+
+int astro_rhs_static(const AstroParams* p, const AstroGrid* g, const double* pr, double* rhs,
+                     void* stream) {
+    int v = validate(p, g);
+    if (v != ASTRO_OK) return v;
+    if (!pr || !rhs) return ASTRO_E_INVALID;
+    const Layout L = layout_of(*p, *g, false);
+    if (L.total > kStaticScratchBytes) return ASTRO_E_WORKSPACE;  // grid too large
+    int err = ASTRO_OK;
+    char* w = (char*)static_scratch_address(&err);
+    if (!w) return err;
+    cudaStream_t s = (cudaStream_t)stream;
+    const Bounds b = bounds_of(*p, *g);
+    // every scratch value the update reads is written by the face passes of
+    // this same call, so nothing has to be cleared first
+    cudaError_t e = face_passes(*p, *g, b, pr, w, L, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    UpdArgs u = update_args(*p, *g, b, w, L);
+    u.pr0 = pr; u.prk = pr; u.dst = rhs; u.rhs_only = 1;
+    return cuda_status(launch_update(u, s));
 }
 
 }  // extern "C"

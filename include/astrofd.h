@@ -118,6 +118,26 @@ size_t astro_rhs_workspace_bytes(const AstroParams* p, const AstroGrid* g);
 int astro_rhs(const AstroParams* p, const AstroGrid* g, const double* pr, double* rhs,
               void* work, size_t work_bytes, void* stream);
 
+/* --- right-hand side without caller scratch --------------------------------
+ * No counterpart in the reference.  Same result as astro_rhs, for callers
+ * that cannot allocate device memory: a host code that binds this library
+ * through an FFI (cgo, Fortran, ctypes) and owns only the primitive and rhs
+ * arrays it passes, with no device allocator of its own to lend scratch from,
+ * or a time-stepping loop that must not call cudaMalloc, which synchronises
+ * the device.  The scratch is a fixed array of astro_rhs_static_max_bytes()
+ * (32 MiB) in the library's device memory, held by every GPU that loads the
+ * library until the process exits.  Grids whose scratch would exceed it are
+ * rejected with ASTRO_E_WORKSPACE (e.g. up to ~48^3 cells including ghosts
+ * for RMHD WENO in float64 reference mode).  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (different streams or
+ * host threads without ordering) race and must be serialised by the caller.
+ * It calls no cudaMalloc/cudaFree. */
+size_t astro_rhs_static_max_bytes(void);
+int astro_rhs_static(const AstroParams* p, const AstroGrid* g, const double* pr, double* rhs,
+                     void* stream);
+
 /* --- one SSPRK step -----------------------------------------------------
  * Replaces {srhd,rmhd}_core.step_ssprk2/3 (core/srhd_core.py:1286,1334;
  * core/rmhd_core.py:1559,1609): returns the new primitive block in pr_out
