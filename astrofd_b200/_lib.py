@@ -28,8 +28,7 @@ class AstroParams(C.Structure):
                 ("riemann", C.c_int32), ("n_passive", C.c_int32),
                 ("passive_offset", C.c_int32), ("resistive", C.c_int32),
                 ("flux_mode", C.c_int32), ("precision", C.c_int32),
-                ("c2p_guess", C.c_int32), ("reserved0", C.c_int32),
-                ("reserved1", C.c_int32), ("gamma", C.c_double),
+                ("c2p_guess", C.c_int32), ("mlp", C.c_void_p), ("gamma", C.c_double),
                 ("srhd_gamma", C.c_double), ("p_max", C.c_double),
                 ("v_max", C.c_double), ("glm_ch", C.c_double), ("glm_cp", C.c_double),
                 ("resistivity", C.c_double)]
@@ -93,6 +92,15 @@ PROTOS = {
                                       _DP, _VP, C.c_int32, _VP]),
     "astro_p2c": (C.c_int, [C.POINTER(AstroParams), _DP, _DP, C.c_int64, _VP]),
     "astro_c2p": (C.c_int, [C.POINTER(AstroParams), _DP, _DP, C.c_int64, _VP, _VP]),
+    "astro_mlp_param_bytes": (C.c_size_t, []),
+    "astro_mlp_trainable": (C.c_int, []),
+    "astro_c2p_features": (C.c_int, [_DP, _DP, C.c_int64, _VP]),
+    "astro_mlp_forward": (C.c_int, [_VP, _DP, _DP, C.c_int64, _VP, _VP]),
+    "astro_mlp_train_grad": (C.c_int, [_VP, _DP, _DP, C.c_int64, _DP, _DP, _VP, _VP]),
+    "astro_mlp_adam": (C.c_int, [_VP, _DP, _DP, _DP, C.c_float, C.c_float, C.c_float,
+                                 C.c_float, C.c_int, _VP]),
+    "astro_c2p_learned": (C.c_int, [C.POINTER(AstroParams), _DP, _DP, C.c_int64, C.c_int,
+                                    _VP, _VP, _VP]),
     "astro_cooling_heating": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, C.c_double,
                                         C.c_double, C.c_double, C.c_double, _VP]),
     "astro_two_temperature": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, C.c_double,

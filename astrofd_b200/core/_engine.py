@@ -30,7 +30,34 @@ class Engine:
         self.p.flux_mode = _lib.FLUX_REFERENCE
         self.p.precision = _lib.PREC_FP64
         self.p.c2p_guess = _lib.GUESS_REFERENCE
+        self.p.mlp = None
+        self.net = None
         self.stats = None
+
+    # -- learned con2prim network ------------------------------------------
+    def set_network(self, params):
+        """Device parameter block of the learned con2prim guess (float32,
+        astro_mlp_param_bytes() bytes), or None."""
+        if params is None:
+            self.net, self.p.mlp = None, None
+            return
+        t = torch.as_tensor(params, dtype=torch.float32)
+        if not t.is_cuda:
+            t = t.cuda()
+        t = t.contiguous()
+        if t.numel() * 4 != _lib.load().astro_mlp_param_bytes():
+            raise _lib.AstroError("network parameter block has the wrong size")
+        self.net = t
+        self.p.mlp = t.data_ptr()
+
+    def _require_network(self):
+        if self.p.c2p_guess == _lib.GUESS_LEARNED and self.net is None:
+            from .. import learned_c2p
+            import os
+            if not os.path.exists(learned_c2p.DATA):
+                raise _lib.AstroError("C2P_GUESS='learned' needs a trained network: "
+                                      "set_c2p_network(...) or python -m astrofd_b200.train_c2p_mlp")
+            self.set_network(learned_c2p.load())
 
     # -- configure() ------------------------------------------------------
     def configure(self, params):
@@ -90,6 +117,7 @@ class Engine:
         nb = L.astro_step_workspace_bytes(C.byref(self.p), C.byref(grid))
         if nb == 0:
             _lib.check(-4, "astro_step (configuration)")
+        self._require_network()
         w = rt.workspace(nb, t.device)
         stats = self._stats_buffer(t.device)
         _lib.check(L.astro_step(C.byref(self.p), C.byref(grid), rt.ptr(t), rt.ptr(out),
@@ -102,6 +130,7 @@ class Engine:
         L = _lib.load()
         grid = rt.grid_of(pr, dx, dy, dz)
         nb = L.astro_step_workspace_bytes(C.byref(self.p), C.byref(grid))
+        self._require_network()
         w = rt.workspace(nb, pr.device)
         stats = self._stats_buffer(pr.device)
         times = _lib.AstroKernelTimes()

@@ -93,6 +93,12 @@ def cons_to_prim_rmhd(D, Sx, Sy, Sz, tau, Bx, By, Bz, psi):
     return _pointwise(_E.c2p_array, (D, Sx, Sy, Sz, tau, Bx, By, Bz, psi))
 
 
+def set_c2p_network(params):
+    """Parameter block of the learned con2prim guess used when
+    C2P_GUESS='learned' (defaults to the packaged trained network)."""
+    _E.set_network(params)
+
+
 def c2p_stats(reset=False):
     return _E.c2p_stats(reset)
 

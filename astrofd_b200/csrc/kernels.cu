@@ -25,6 +25,7 @@
 #include <atomic>
 #include <mutex>
 
+#include "mlp.cuh"
 #include "physics.cuh"
 
 using namespace astro;
@@ -76,7 +77,7 @@ __host__ Bounds bounds_of(const AstroParams& p, const AstroGrid& g) {
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
-    size_t prA, prB, U, F[3], FxC, aux[3], Sz, total;
+    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, total;
 };
 
 inline bool carried_mode(const AstroParams& p) {
@@ -88,6 +89,13 @@ inline bool passive_fluxes(const AstroParams& p) {
     if (p.n_passive <= 0) return false;
     if (p.physics == ASTRO_SRHD) return p.recon != ASTRO_RECON_WENO;
     return p.recon == ASTRO_RECON_MUSCL;
+}
+
+// capacity of the float64 fix-up list: a fraction of one face pass; faces
+// beyond it keep their float32 result (counted, never written out of bounds)
+inline size_t fix_capacity(const AstroGrid& g) {
+    const size_t nc = (size_t)g.nx * g.ny * g.nz;
+    return nc / 16 + 1024;
 }
 
 Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
@@ -104,6 +112,8 @@ Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
     L.FxC = carried_mode(p) ? take((size_t)nm * nc * rs) : 0;
     for (int d = 0; d < 3; ++d) L.aux[d] = passive_fluxes(p) ? take(4 * nc * rs) : 0;
     L.Sz = carried_mode(p) ? take(2 * nc * rs) : 0;
+    // float32 passes: counter + list of faces to recompute in float64
+    L.fix = p.precision == ASTRO_PREC_MIXED ? take(256 + fix_capacity(g) * sizeof(unsigned)) : 0;
     L.total = o;
     return L;
 }
@@ -142,22 +152,21 @@ struct FaceArgs {
     void* speeds_out;    // R[2][nc]: sL, sR (z faces, carried mode) or null
     const void* carried; // R[2][nc]: z-face speeds read by the carried x faces
     AstroParams p;
+    // float32 passes: faces whose float32 result is not finite are listed here
+    // and recomputed in float64 by k_face_fix
+    unsigned* fix_count;
+    unsigned* fix_list;
+    unsigned fix_cap;
 };
 
-template <int PHYS, int RECON, int RIEMANN, typename R, bool GIVEN>
-__global__ void __launch_bounds__(128) k_face(FaceArgs a) {
+// One face: reconstruct, floor, p2c, flux, speeds, Riemann in arithmetic R,
+// stored as RS.  Returns false when the stored flux or speeds are not finite.
+template <int PHYS, int RECON, int RIEMANN, typename R, typename RS, bool GIVEN, int DIR>
+__device__ __forceinline__ bool face_at(const FaceArgs& a, int i, int j, int k) {
     constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
-    const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const int c = (int)(t % a.ext[2]);
-    const long r = t / a.ext[2];
-    const int bb = (int)(r % a.ext[1]);
-    const int aa = (int)(r / a.ext[1]);
-    const int i = a.org[0] + aa, j = a.org[1] + bb, k = a.org[2] + c;
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
     const size_t cell = ((size_t)i * a.ny + j) * a.nz + k;
-    const long stride = a.dir == 0 ? (long)a.ny * a.nz : (a.dir == 1 ? (long)a.nz : 1L);
+    const long stride = DIR == 0 ? (long)a.ny * a.nz : (DIR == 1 ? (long)a.nz : 1L);
     const Phys<R> P = Phys<R>::from(a.p);
 
     R qL[NM], qR[NM];
@@ -165,11 +174,11 @@ __global__ void __launch_bounds__(128) k_face(FaceArgs a) {
     constexpr int o1 = RECON == ASTRO_RECON_MUSCL ? 1 : 2;
 #pragma unroll
     for (int v = 0; v < NM; ++v) {
-        R s[6];
+        R st[6];
         const double* base = a.pr + (size_t)v * nc + cell;
 #pragma unroll
-        for (int o = o0; o <= o1; ++o) s[o + 3] = (R)__ldg(base + o * stride);
-        recon_face<RECON>(s, a.p.limiter, qL[v], qR[v]);
+        for (int o = o0; o <= o1; ++o) st[o + 3] = (R)__ldg(base + o * stride);
+        recon_face<RECON>(st, a.p.limiter, qL[v], qR[v]);
     }
     R F[NM];
     R sL = R(-1), sR = R(1);
@@ -183,31 +192,72 @@ __global__ void __launch_bounds__(128) k_face(FaceArgs a) {
         else if (i > a.b.lo) { pi = i - 1; pj = a.b.hi[1] - 1; pk = a.b.hi[2] - 1; }
         else first = true;
         if (!first) {
-            const R* S = (const R*)a.carried;
+            const RS* S = (const RS*)a.carried;
             const size_t pc = ((size_t)pi * a.ny + pj) * a.nz + pk;
-            sL = S[pc];
-            sR = S[nc + pc];
+            sL = (R)S[pc];
+            sR = (R)S[nc + pc];
         }
     }
     if (PHYS == ASTRO_SRHD) {
-        s_face<RIEMANN>(P, a.dir, qL, qR, F, sL, sR);
+        s_face<RIEMANN>(P, DIR, qL, qR, F, sL, sR);
     } else {
-        r_face<RIEMANN, RECON == ASTRO_RECON_MUSCL, GIVEN>(P, a.dir, qL, qR, F, sL, sR);
+        r_face<RIEMANN, RECON == ASTRO_RECON_MUSCL, GIVEN>(P, DIR, qL, qR, F, sL, sR);
     }
-    R* Fo = (R*)a.F;
+    RS* Fo = (RS*)a.F;
+    bool finite = true;
 #pragma unroll
-    for (int v = 0; v < NM; ++v) Fo[(size_t)v * nc + cell] = F[v];
+    for (int v = 0; v < NM; ++v) {
+        const RS f = (RS)F[v];
+        finite &= isfinite(f);
+        Fo[(size_t)v * nc + cell] = f;
+    }
+    finite &= isfinite((RS)sL) && isfinite((RS)sR);
     if (a.aux) {
-        R* A = (R*)a.aux;
-        A[cell] = sL;
-        A[nc + cell] = sR;
-        A[2 * nc + cell] = qL[1 + a.dir];
-        A[3 * nc + cell] = qR[1 + a.dir];
+        RS* A = (RS*)a.aux;
+        A[cell] = (RS)sL;
+        A[nc + cell] = (RS)sR;
+        A[2 * nc + cell] = (RS)qL[1 + DIR];
+        A[3 * nc + cell] = (RS)qR[1 + DIR];
     }
     if (a.speeds_out) {
-        R* S = (R*)a.speeds_out;
-        S[cell] = sL;
-        S[nc + cell] = sR;
+        RS* S = (RS*)a.speeds_out;
+        S[cell] = (RS)sL;
+        S[nc + cell] = (RS)sR;
+    }
+    return finite;
+}
+
+template <int PHYS, int RECON, int RIEMANN, typename R, bool GIVEN, int DIR>
+__global__ void __launch_bounds__(128) k_face(FaceArgs a) {
+    const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int c = (int)(t % a.ext[2]);
+    const long r = t / a.ext[2];
+    const int bb = (int)(r % a.ext[1]);
+    const int aa = (int)(r / a.ext[1]);
+    const int i = a.org[0] + aa, j = a.org[1] + bb, k = a.org[2] + c;
+    const bool ok = face_at<PHYS, RECON, RIEMANN, R, R, GIVEN, DIR>(a, i, j, k);
+    if (sizeof(R) == 4 && !ok && a.fix_list) {
+        const unsigned slot = atomicAdd(a.fix_count, 1u);
+        if (slot < a.fix_cap) a.fix_list[slot] = (unsigned)t;
+    }
+}
+
+// float64 recomputation of the faces a float32 pass listed as non-finite
+// (float32 overflows where float64 does not, e.g. squared WENO smoothness
+// indicators of a state whose fields have grown past ~1e9)
+template <int PHYS, int RECON, int RIEMANN, bool GIVEN, int DIR>
+__global__ void __launch_bounds__(128) k_face_fix(FaceArgs a) {
+    const unsigned n = min(*a.fix_count, a.fix_cap);
+    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        const long t = a.fix_list[q];
+        const int c = (int)(t % a.ext[2]);
+        const long r = t / a.ext[2];
+        const int bb = (int)(r % a.ext[1]);
+        const int aa = (int)(r / a.ext[1]);
+        face_at<PHYS, RECON, RIEMANN, double, float, GIVEN, DIR>(a, a.org[0] + aa, a.org[1] + bb,
+                                                                a.org[2] + c);
     }
 }
 
@@ -224,6 +274,7 @@ struct UpdArgs {
     Bounds b;
     double dd[3], dt;
     int stage, nstages, rhs_only;
+    int defer_c2p;       // learned con2prim: write U every stage, primitives later
     AstroParams p;
     AstroC2PStats* stats;
 };
@@ -262,7 +313,9 @@ template <typename RF> __device__ __forceinline__ double ldf(const void* p, size
     return (double)__ldg((const RF*)p + i);
 }
 
-template <int PHYS, typename RF>
+// DEFER: the learned con2prim runs in its own kernel, so this one only
+// writes U (the con2prim code is compiled out, which frees registers).
+template <int PHYS, typename RF, bool DEFER, bool PASSIVE>
 __global__ void __launch_bounds__(128) k_update(UpdArgs a) {
     constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
@@ -317,7 +370,7 @@ __global__ void __launch_bounds__(128) k_update(UpdArgs a) {
                 }
             }
             // passive scalars: the reference's triple evaluation (see header)
-            if (np > 0) {
+            if (PASSIVE && np > 0) {
                 for (int n = 0; n < 3; ++n) {
                     int kinds[3], nk = 0, lkind = PK_MC;
                     if (PHYS == ASTRO_SRHD) {
@@ -378,14 +431,16 @@ __global__ void __launch_bounds__(128) k_update(UpdArgs a) {
                 }
                 Un[v] = un;
             }
-            if (a.stage != a.nstages - 1) {
+            if (a.stage != a.nstages - 1 || DEFER) {
 #pragma unroll
                 for (int v = 0; v < NM; ++v) a.U[(size_t)v * nc + cell] = Un[v];
             }
-            if (PHYS == ASTRO_SRHD) s_c2p(P, Un, q);
-            else r_c2p(P, Un, q, cnt);
+            if (!DEFER) {
+                if (PHYS == ASTRO_SRHD) s_c2p(P, Un, q);
+                else r_c2p(P, Un, q, cnt);
 #pragma unroll
-            for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = q[v];
+                for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = q[v];
+            }
             for (int v = NM; v < a.nv; ++v) {
                 double out = 0.0;
                 const int t = v - po;
@@ -408,7 +463,7 @@ __global__ void __launch_bounds__(128) k_update(UpdArgs a) {
             }
         }
     }
-    if (a.stats && !a.rhs_only) {
+    if (!DEFER && a.stats && !a.rhs_only) {
         // warp-aggregated counters, one atomic per warp and counter
         unsigned n1 = __reduce_add_sync(0xffffffffu, cell < nc ? 1u : 0u);
         unsigned n2 = __reduce_add_sync(0xffffffffu, cnt.newton);
@@ -423,18 +478,189 @@ __global__ void __launch_bounds__(128) k_update(UpdArgs a) {
     }
 }
 
+// ------------------------------------------------- learned con2prim ---
+// Five invariants of a conserved RMHD state (log D, |S|/D, tau/D, B^2/D,
+// (S.B)^2/D^3), the last four through log1p so the inputs stay O(1).
+__device__ __forceinline__ void c2p_features(const double* U, float* x) {
+    const double D = rmax(U[0], 1e-300);
+    const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+    const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+    const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
+    const double r[4] = {sqrt(S2) / D, rmax(U[4], 0.0) / D, B2 / D, SB * SB / (D * D * D)};
+    x[0] = (float)log(D);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x[1 + i] = log1pf((float)rmin(r[i], 1e30));
+}
+
+struct C2PArgs {
+    const double* U;   // [9][count]
+    double* q;         // [>=9][count]: rows 0..8 written
+    long count;
+    AstroParams p;
+    const mlp::Params* net;
+    AstroC2PStats* stats;
+    int* status;
+    int max_polish;
+};
+
+// Learned con2prim: per 128-cell tile the MLP (tcgen05, BF16, FP32 accumulate)
+// predicts (log W, log p); Z = D W + Gamma/(Gamma-1) p W^2 starts at most
+// max_polish Newton steps of the reference's update; cells that do not meet
+// |f| < 1e-10 max(1, tau) continue with the full Newton solve from there and,
+// failing that, run the reference's complete con2prim.
+__global__ void __launch_bounds__(128) k_c2p_learned(C2PArgs a) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + mlp::kInferSmem);
+    uint32_t* taddr_s = reinterpret_cast<uint32_t*>(sm + mlp::kInferSmem + 8);
+    const int t = threadIdx.x;
+    const bool net = a.net != nullptr;  // uniform; without a network: Z = D + tau + B^2
+    if (net) {
+        if (t < 32) mlp::tmem_alloc(mlp::smem_u32(taddr_s), 64);
+        if (t == 0) mlp::mbar_init_fenced(mlp::smem_u32(bar), 1);
+        mlp::load_weights(sm, a.net);
+        mlp::fence_async_smem();
+        mlp::tc_fence_before();
+    }
+    __syncthreads();
+    if (net) mlp::tc_fence_after();
+    const uint32_t tmem = net ? *taddr_s : 0u;
+    uint32_t phase = 0;
+    const Phys<double> P = Phys<double>::from(a.p);
+    const double gfac = a.p.gamma / (a.p.gamma - 1.0);
+    C2PCount cnt;
+    unsigned n_cells = 0, n_polish = 0, n_fallback = 0, polish_steps = 0;
+    const long ntiles = (a.count + mlp::TILE - 1) / mlp::TILE;
+    for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long cell = tile * mlp::TILE + t;
+        const bool valid = cell < a.count;
+        double U[9] = {1, 0, 0, 0, 1, 0, 0, 0, 0};
+        if (valid)
+#pragma unroll
+            for (int v = 0; v < 9; ++v) U[v] = a.U[(size_t)v * a.count + cell];
+        float o[2] = {0.f, 0.f};
+        if (net) {
+            float xr[5], h0[5];
+            c2p_features(U, xr);
+            mlp::features_norm(a.net, xr, h0);
+            if (!mlp::forward_tile<false>(sm, tmem, mlp::smem_u32(bar), phase, a.net, h0, o,
+                                          a.status))
+                break;
+        }
+        if (!valid) continue;
+        ++n_cells;
+        const double D = U[0], tau = U[4];
+        const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+        const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
+        const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+        double Z;
+        if (net) {
+            const double logW = rmax((double)(o[0] * a.net->ysd[0] + a.net->ymu[0]), 0.0);
+            const double logp = (double)(o[1] * a.net->ysd[1] + a.net->ymu[1]);
+            const double W = exp(rmin(logW, 20.0)), pg = exp(rmax(rmin(logp, 50.0), -60.0));
+            Z = rmax(D * W + gfac * pg * W * W, 1e-12);
+        } else {
+            Z = rmax(D + tau + B2, 1e-12);
+        }
+        double q[9];
+        int steps = 0;
+        bool done = false;
+        if (isfinite(Z) && r_newton_polish(P, Z, a.max_polish, D, tau, B2, SB, S2, &steps)) {
+            ++n_polish;
+            polish_steps += steps;
+            done = r_prims_from_Z_checked(P, Z, U, q);
+        } else {
+            ++n_fallback;
+            polish_steps += a.max_polish;
+            if (isfinite(Z) && r_newton(P, Z, 50, D, tau, B2, SB, S2)) {
+                cnt.newton++;
+                done = r_prims_from_Z_checked(P, Z, U, q);
+            }
+        }
+        if (!done) r_c2p(P, U, q, cnt);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
+    }
+    if (net) {
+        mlp::tc_fence_before();
+        __syncthreads();
+        if (t < 32) mlp::tmem_free(tmem, 64);
+    }
+    if (a.stats) {
+        atomicAdd(&a.stats->cells, (unsigned long long)n_cells);
+        if (n_polish) atomicAdd(&a.stats->learned_polish, (unsigned long long)n_polish);
+        if (n_fallback) atomicAdd(&a.stats->learned_fallback, (unsigned long long)n_fallback);
+        if (polish_steps) atomicAdd(&a.stats->polish_steps, (unsigned long long)polish_steps);
+        if (cnt.newton) atomicAdd(&a.stats->newton, (unsigned long long)cnt.newton);
+        if (cnt.bisect) atomicAdd(&a.stats->bisection, (unsigned long long)cnt.bisect);
+        if (cnt.hydro_fallback) atomicAdd(&a.stats->hydro_fallback, (unsigned long long)cnt.hydro_fallback);
+    }
+}
+
+__global__ void k_c2p_features(const double* U, float* x, long count) {
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long)gridDim.x * blockDim.x) {
+        double u[9];
+        for (int v = 0; v < 9; ++v) u[v] = U[(size_t)v * count + t];
+        float f[5];
+        c2p_features(u, f);
+        for (int i = 0; i < 5; ++i) x[t * 5 + i] = f[i];
+    }
+}
+
+int g_sm_count = 0;
+int sm_count_cached() {
+    if (!g_sm_count) {
+        int dev = 0, n = 148;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        g_sm_count = n;
+    }
+    return g_sm_count;
+}
+
+cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
+    const long ntiles = (a.count + mlp::TILE - 1) / mlp::TILE;
+    const long cap = 4L * sm_count_cached();
+    const int grid = (int)(ntiles < cap ? ntiles : cap);
+    if (grid <= 0) return cudaSuccess;
+    k_c2p_learned<<<grid, mlp::TILE, mlp::kInferSmem + 16, s>>>(a);
+    mark(1, s);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------- dispatch ---
+// direction is a template parameter so the per-direction component indices
+// fold to constants and the face state stays in registers
+template <int PH, int RE, int RI, typename R>
+void launch_face_dir(const FaceArgs& a, bool given, dim3 grd, dim3 blk, cudaStream_t s) {
+    constexpr bool F32 = sizeof(R) == 4;
+    const dim3 fgrd(148 * 4);
+    if (F32) cudaMemsetAsync(a.fix_count, 0, sizeof(unsigned), s);
+    if constexpr (PH == ASTRO_RMHD && RE != ASTRO_RECON_MUSCL) {
+        if (given) {
+            k_face<PH, RE, RI, R, true, 0><<<grd, blk, 0, s>>>(a);
+            if (F32) k_face_fix<PH, RE, RI, true, 0><<<fgrd, blk, 0, s>>>(a);
+            return;
+        }
+    }
+    if (a.dir == 0) {
+        k_face<PH, RE, RI, R, false, 0><<<grd, blk, 0, s>>>(a);
+        if (F32) k_face_fix<PH, RE, RI, false, 0><<<fgrd, blk, 0, s>>>(a);
+    } else if (a.dir == 1) {
+        k_face<PH, RE, RI, R, false, 1><<<grd, blk, 0, s>>>(a);
+        if (F32) k_face_fix<PH, RE, RI, false, 1><<<fgrd, blk, 0, s>>>(a);
+    } else {
+        k_face<PH, RE, RI, R, false, 2><<<grd, blk, 0, s>>>(a);
+        if (F32) k_face_fix<PH, RE, RI, false, 2><<<fgrd, blk, 0, s>>>(a);
+    }
+}
+
 template <typename R>
 cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
     const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
     if (total <= 0) return cudaSuccess;
     const dim3 blk(128), grd((unsigned)((total + 127) / 128));
     const AstroParams& p = a.p;
-#define FACE(PH, RE, RI)                                                        \
-    do {                                                                        \
-        if (given) k_face<PH, RE, RI, R, true><<<grd, blk, 0, s>>>(a);          \
-        else k_face<PH, RE, RI, R, false><<<grd, blk, 0, s>>>(a);               \
-    } while (0)
+#define FACE(PH, RE, RI) launch_face_dir<PH, RE, RI, R>(a, given, grd, blk, s)
 #define RECONS(PH, RI)                                                          \
     do {                                                                        \
         if (p.recon == 0) FACE(PH, 0, RI);                                      \
@@ -459,13 +685,21 @@ cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
     const dim3 blk(128), grd((unsigned)((nc + 127) / 128));
     const bool mixed = a.p.precision == ASTRO_PREC_MIXED;
-    if (a.p.physics == ASTRO_SRHD) {
-        if (mixed) k_update<ASTRO_SRHD, float><<<grd, blk, 0, s>>>(a);
-        else k_update<ASTRO_SRHD, double><<<grd, blk, 0, s>>>(a);
-    } else {
-        if (mixed) k_update<ASTRO_RMHD, float><<<grd, blk, 0, s>>>(a);
-        else k_update<ASTRO_RMHD, double><<<grd, blk, 0, s>>>(a);
-    }
+    const bool pas = passive_fluxes(a.p);
+#define UPD(PH, DEF)                                                               \
+    do {                                                                           \
+        if (pas) {                                                                 \
+            if (mixed) k_update<PH, float, DEF, true><<<grd, blk, 0, s>>>(a);      \
+            else k_update<PH, double, DEF, true><<<grd, blk, 0, s>>>(a);           \
+        } else {                                                                   \
+            if (mixed) k_update<PH, float, DEF, false><<<grd, blk, 0, s>>>(a);     \
+            else k_update<PH, double, DEF, false><<<grd, blk, 0, s>>>(a);          \
+        }                                                                          \
+    } while (0)
+    if (a.p.physics == ASTRO_SRHD) UPD(ASTRO_SRHD, false);
+    else if (a.defer_c2p) UPD(ASTRO_RMHD, true);
+    else UPD(ASTRO_RMHD, false);
+#undef UPD
     mark(1, s);
     return cudaGetLastError();
 }
@@ -487,6 +721,11 @@ cudaError_t face_passes(const AstroParams& p, const AstroGrid& g, const Bounds& 
         }
         a.F = work + L.F[d];
         a.aux = passive_fluxes(p) ? (void*)(work + L.aux[d]) : nullptr;
+        if (mixed) {
+            a.fix_count = (unsigned*)(work + L.fix);
+            a.fix_list = (unsigned*)(work + L.fix + 256);
+            a.fix_cap = (unsigned)fix_capacity(g);
+        }
         a.speeds_out = (carried && d == 2) ? (void*)(work + L.Sz) : nullptr;
         cudaError_t e = mixed ? launch_face_t<float>(a, false, s) : launch_face_t<double>(a, false, s);
         if (e != cudaSuccess) return e;
@@ -829,7 +1068,9 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
     if (v != ASTRO_OK) return v;
     if (!pr_in || !pr_out || pr_in == pr_out) return ASTRO_E_INVALID;
     if (rk_order != 2 && rk_order != 3) return ASTRO_E_INVALID;
-    if (p->c2p_guess != ASTRO_GUESS_REFERENCE) return ASTRO_E_UNSUPPORTED;
+    const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
+    if (p->c2p_guess != ASTRO_GUESS_REFERENCE && !learned) return ASTRO_E_INVALID;
+    if (learned && (p->physics != ASTRO_RMHD || !p->mlp)) return ASTRO_E_UNSUPPORTED;
     const Layout L = layout_of(*p, *g, true);
     if (!work || work_bytes < L.total) return ASTRO_E_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
@@ -845,8 +1086,18 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
         UpdArgs u = update_args(*p, *g, b, w, L);
         u.pr0 = pr_in; u.prk = cur; u.U = (double*)(w + L.U); u.dst = dst;
         u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
+        u.defer_c2p = learned ? 1 : 0;
         e = launch_update(u, s);
         if (e != cudaSuccess) return ASTRO_E_CUDA;
+        if (learned) {
+            C2PArgs c;
+            c.U = (const double*)(w + L.U); c.q = dst;
+            c.count = (long)g->nx * g->ny * g->nz;
+            c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
+            c.status = nullptr; c.max_polish = 2;
+            e = launch_c2p_learned(c, s);
+            if (e != cudaSuccess) return ASTRO_E_CUDA;
+        }
         cur = dst;
     }
     return ASTRO_OK;
@@ -974,6 +1225,26 @@ int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, dou
     const size_t n = (size_t)(g->nx - 2 * ng) * (g->ny - 2 * ng) * (g->nz - 2 * ng);
     k_two_temperature<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
         pr, g->nx, g->ny, g->nz, ng, dt, tau, thermo_offset);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
+                      int max_polish, AstroC2PStats* stats, int* status, void* stream) {
+    if (!p || !cons || !prim || count < 0 || p->physics != ASTRO_RMHD) return ASTRO_E_INVALID;
+    if (max_polish < 0 || max_polish > 50) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;
+    C2PArgs c;
+    c.U = cons; c.q = prim; c.count = count; c.p = *p;
+    c.net = (const mlp::Params*)p->mlp; c.stats = stats; c.status = status;
+    c.max_polish = max_polish;
+    return cuda_status(launch_c2p_learned(c, (cudaStream_t)stream));
+}
+
+int astro_c2p_features(const double* cons, float* x, int64_t count, void* stream) {
+    if (!cons || !x || count < 0) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;
+    k_c2p_features<<<grid_for(count, 256), 256, 0, (cudaStream_t)stream>>>(cons, x, count);
     mark(2, (cudaStream_t)stream);
     return cuda_status(cudaGetLastError());
 }

@@ -643,6 +643,64 @@ AHD void r_c2p_start(const Phys<double>& P, const double* U, double* q0, double&
     Z1 = rmax(D + tau + B2, SM);
 }
 
+// At most max_steps Newton steps of the reference's update rule (forward-
+// difference derivative, +-Z/2 clamp), testing |f| < 1e-10 max(1, tau) before
+// each step and after the last.  *steps = steps taken when converged.
+AHD bool r_newton_polish(const Phys<double>& P, double& Z, int max_steps, double D, double tau,
+                         double B2, double SB, double S2, int* steps) {
+    const double tol = 1e-10 * rmax(1.0, tau);
+    for (int s = 0;; ++s) {
+        double f = r_f_of_Z(P, Z, D, tau, B2, SB, S2);
+        if (fabs(f) < tol) {
+            *steps = s;
+            return true;
+        }
+        if (s == max_steps) break;
+        double eps = 1e-6 * rmax(1.0, Z);
+        double fp = r_f_of_Z(P, Z + eps, D, tau, B2, SB, S2);
+        double dfdZ = (fp - f) / eps;
+        if (dfdZ == 0.0) break;
+        double dZ = -f / dfdZ;
+        if (dZ > 0.5 * Z) dZ = 0.5 * Z;
+        if (dZ < -0.5 * Z) dZ = -0.5 * Z;
+        Z += dZ;
+        if (Z < 1e-12) Z = 1e-12;
+    }
+    *steps = max_steps;
+    return false;
+}
+
+// Primitives from a converged Z (rmhd_core.py:320-341) without the hydro
+// fallback: returns false when the result is invalid (the caller then runs
+// the reference's full con2prim, which owns that fallback).
+AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U, double* q) {
+    const double G = P.gamma, SM = 1e-12;
+    double Sx = U[1], Sy = U[2], Sz = U[3], D = U[0];
+    double Bx = U[5], By = U[6], Bz = U[7];
+    double B2 = Bx * Bx + By * By + Bz * Bz;
+    double SB = Sx * Bx + Sy * By + Sz * Bz;
+    double ZpB = Z + B2;
+    double vb = SB / rmax(Z, SM);
+    double vx = (Sx + vb * Bx) / rmax(ZpB, SM);
+    double vy = (Sy + vb * By) / rmax(ZpB, SM);
+    double vz = (Sz + vb * Bz) / rmax(ZpB, SM);
+    double v2 = vx * vx + vy * vy + vz * vz;
+    double vmax2 = P.v_max * P.v_max;
+    if (v2 >= vmax2) {
+        double fac = P.v_max / sqrt(v2 + 1e-32);
+        vx *= fac; vy *= fac; vz *= fac;
+    }
+    double W = 1.0 / sqrt(1.0 - (vx * vx + vy * vy + vz * vz));
+    double rho = D / rmax(W, SM);
+    double h = Z / rmax(rho * W * W, SM);
+    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    if (!isfinite(rho) || !isfinite(p) || rho <= 0.0 || p <= 0.0) return false;
+    q[0] = rho; q[1] = vx; q[2] = vy; q[3] = vz; q[4] = p;
+    q[5] = Bx; q[6] = By; q[7] = Bz; q[8] = U[8];
+    floor_prim(P, q);
+    return true;
+}
+
 // Full reference con2prim (cons_to_prim_rmhd, rmhd_core.py:249-341)
 AHD void r_c2p(const Phys<double>& P, const double* U, double* q, C2PCount& cnt) {
     double D = U[0], tau = U[4];

@@ -53,6 +53,14 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-x-cells", type=int, default=4,
                     help="x-slab thickness of the bounded CPU sample")
+    ap.add_argument("--c2p-net", default=None,
+                    help="learned con2prim weights (.npz); default: the packaged network")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="headline arm without the learned con2prim guess")
+    ap.add_argument("--validate-steps", type=int, default=0,
+                    help="instead of timing: run this many steps of mixed+learned, plain "
+                         "float64 and float64 with a 1e-12 density perturbation and report "
+                         "density L1 errors and conservative-mode mass drift")
     return ap.parse_args()
 
 
@@ -178,13 +186,17 @@ class DriverStep:
         return out, pr, times
 
 
-def time_arm(args, world, prec, pr_host, cfgs, profile):
+def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     import torch
     from astrofd_b200 import _lib
     from astrofd_b200.core import rmhd_core
     core, noz, src = cfgs
-    cfg = dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode)
+    cfg = dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
+               C2P_GUESS="learned" if learned else "reference")
     rmhd_core.configure(cfg)
+    if learned:
+        from astrofd_b200 import learned_c2p
+        rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
     step = DriverStep(args.n, 3, core, noz, src)
     a = torch.from_numpy(pr_host).to("cuda")
     b = torch.empty_like(a)
@@ -217,13 +229,17 @@ def time_arm(args, world, prec, pr_host, cfgs, profile):
                 clocks=clk.summary(), finite=finite, state=a, c2p=stats)
 
 
-def time_e2e(args, world, prec, pr_host, cfgs):
+def time_e2e(args, world, prec, pr_host, cfgs, learned=False):
     """Public API with host buffers: each step uploads the block from pinned
     host memory and reads the result back."""
     import torch
     from astrofd_b200.core import rmhd_core
     core, noz, src = cfgs
-    rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode))
+    rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
+                             C2P_GUESS="learned" if learned else "reference"))
+    if learned:
+        from astrofd_b200 import learned_c2p
+        rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
     step = DriverStep(args.n, 3, core, noz, src)
     host_in = torch.from_numpy(pr_host).pin_memory()
     host_out = torch.empty_like(host_in).pin_memory()
@@ -337,8 +353,66 @@ def roofline(args, prof_ms, prof_n, prec):
             "class_share": round(float(prof_ms[cls] / max(prof_ms.sum(), 1e-30)), 3)}
 
 
+def validate(args):
+    """Accuracy protocol of the mixed + learned path against plain float64."""
+    import torch
+    from astrofd_b200 import learned_c2p
+    from astrofd_b200.core import rmhd_core
+    from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
+    n, K = args.n, args.validate_steps
+    cfgs = rmhd_jet_config(n, 3)
+    core, noz, src = cfgs
+
+    def run(prec, learned, perturb=0.0):
+        rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
+                                 C2P_GUESS="learned" if learned else "reference"))
+        if learned:
+            rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
+        pr = rmhd_jet(n, 3)
+        if perturb:
+            pr[0] *= 1.0 + perturb * np.random.default_rng(5).standard_normal(pr[0].shape)
+        step = DriverStep(n, 3, core, noz, src)
+        a = torch.from_numpy(pr).cuda()
+        b = torch.empty_like(a)
+        rmhd_core.c2p_stats(reset=True)
+        for _ in range(K):
+            a, b, _ = step(a, b)
+        return a, rmhd_core.c2p_stats(reset=True)
+
+    ref, st_ref = run("fp64", False)
+    mix, st_mix = run("mixed", True)
+    per, _ = run("fp64", False, perturb=1e-12)
+    i = slice(3, -3)
+
+    def l1(a, b):
+        return float(((a[0, i, i, i] - b[0, i, i, i]).abs().mean() / b[0, i, i, i].abs().mean()).item())
+
+    out = {"validate_steps": K, "grid": n, "flux_mode": args.flux_mode,
+           "rho_l1_mixed_learned_vs_fp64": l1(mix, ref),
+           "rho_l1_fp64_perturbed_1e-12_vs_fp64": l1(per, ref),
+           "c2p_fp64": st_ref, "c2p_mixed_learned": st_mix}
+    # mass: one conservative step of the same state with nothing crossing the
+    # faces of the update region (ambient at rest there) keeps sum(D) to round-off
+    rmhd_core.configure(dict(core, PRECISION="fp64", FLUX_MODE="conservative",
+                             C2P_GUESS="reference"))
+    a = torch.from_numpy(rmhd_jet(n, 3)).cuda()
+    a[1:4] = 0.0  # medium at rest outside the moving cube
+    c = slice(n // 2 - n // 8, n // 2 + n // 8)
+    a[0, c, c, c] = 0.1
+    a[1, c, c, c] = 0.995
+    d = 1.0 / n
+    W = lambda q: 1.0 / torch.sqrt(1.0 - (q[1] ** 2 + q[2] ** 2 + q[3] ** 2))
+    m0 = (a[0] * W(a)).sum().item()
+    b = rmhd_core.step_ssprk3(a, d, d, d, core["CFL"] * d)
+    out["mass_rel_change_one_conservative_step"] = abs((b[0] * W(b)).sum().item() - m0) / m0
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.validate_steps:
+        validate(args)
+        return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
@@ -366,9 +440,10 @@ def main():
     pr_host = rmhd_jet(n, 3, seed=2024 + rank)
     zones = n ** 3 * args.steps * world
 
-    mixed = time_arm(args, world, "mixed", pr_host, cfgs, profile=True)
+    learned = not args.no_learned
+    mixed = time_arm(args, world, "mixed", pr_host, cfgs, profile=True, learned=learned)
     fp64 = None if args.no_fp64 else time_arm(args, world, "fp64", pr_host, cfgs, profile=False)
-    e2e = None if args.no_e2e else time_e2e(args, world, "mixed", pr_host, cfgs)
+    e2e = None if args.no_e2e else time_e2e(args, world, "mixed", pr_host, cfgs, learned=learned)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample(args, steps=1, warmup=0)
@@ -387,7 +462,8 @@ def main():
         "config": {"workload": f"rmhd-jet-{n}^3 weno5/hlld ssprk3 + resistive 1e-4 + "
                                "two-temperature + cooling (driver-loop iteration)",
                    "grid": [n, n, n], "ng": 3, "nv": 11, "precision": "mixed",
-                   "c2p_guess": "reference", "flux_mode": args.flux_mode,
+                   "c2p_guess": "learned" if learned else "reference",
+                   "flux_mode": args.flux_mode,
                    "l2": "inputs larger than L2 (1.6 GB arrays)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "gpu_launches": mixed["launches"],

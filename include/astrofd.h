@@ -70,7 +70,10 @@ extern "C" {
 typedef struct AstroParams {
     int32_t physics, recon, limiter, riemann;
     int32_t n_passive, passive_offset, resistive, flux_mode;
-    int32_t precision, c2p_guess, reserved0, reserved1;
+    int32_t precision, c2p_guess;
+    const void* mlp;     /* device pointer to the learned-guess network's
+                            parameter block (astro_mlp_param_bytes() bytes),
+                            used when c2p_guess == ASTRO_GUESS_LEARNED        */
     double gamma;        /* RMHD adiabatic index (GAMMA)                      */
     double srhd_gamma;   /* SRHD kernels: the reference freezes this at 5/3   */
     double p_max, v_max, glm_ch, glm_cp, resistivity;
@@ -195,6 +198,36 @@ int astro_p2c(const AstroParams* p, const double* prim, double* cons, int64_t co
               void* stream);
 int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t count,
               AstroC2PStats* stats, void* stream);
+
+/* --- learned con2prim initial guess (no counterpart in the reference) ------
+ * A 5-64-64-64-2 SiLU network on the invariants (log D, log1p|S|/D,
+ * log1p tau/D, log1p B^2/D, log1p (S.B)^2/D^3) predicts (log W, log p); the
+ * resulting Z = D W + Gamma/(Gamma-1) p W^2 starts at most max_polish Newton
+ * steps of the reference's update (core/rmhd_core.py:268-292).  Cells whose
+ * residual is still >= 1e-10 max(1, tau) continue with the full Newton solve
+ * and then, if needed, the reference's complete con2prim.  Evaluation and
+ * training use tcgen05 tensor cores (BF16 operands, FP32 accumulation).
+ * The parameter block is float32: W1[64x5] b1[64] W2[64x64] b2[64] W3[64x64]
+ * b3[64] W4[2x64] b4[2] (the astro_mlp_trainable() trainable floats), then
+ * xmu[5] xsd[5] ymu[2] ysd[2] (feature / target normalisation).  `status`
+ * (device int, may be NULL) is set to 1 if a tensor-core wait timed out. */
+size_t astro_mlp_param_bytes(void);
+int astro_mlp_trainable(void);
+int astro_c2p_features(const double* cons, float* x, int64_t count, void* stream);
+int astro_mlp_forward(const void* params, const float* x, float* y, int64_t n, int* status,
+                      void* stream);
+/* adds d(mean squared error)/d(params) over the n samples into grad
+ * (astro_mlp_trainable() floats) and the mean squared error into *loss */
+int astro_mlp_train_grad(const void* params, const float* x, const float* t, int64_t n,
+                         float* grad, float* loss, int* status, void* stream);
+/* one Adam step on the trainable prefix of params; zeroes grad */
+int astro_mlp_adam(void* params, float* grad, float* m, float* v, float lr, float beta1,
+                   float beta2, float eps, int step, void* stream);
+/* con2prim of a (9, count) batch with the learned guess (p->mlp set); with
+ * p->mlp == NULL the same polish/fallback runs from Z = D + tau + B^2 (the
+ * reference's second Newton start), the no-network comparison */
+int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
+                      int max_polish, AstroC2PStats* stats, int* status, void* stream);
 
 /* --- operator-split post-step sources (core/source_terms.py:5,30) -------- */
 int astro_cooling_heating(double* pr, const AstroGrid* g, int ng, double dt, double cool,

@@ -1,0 +1,129 @@
+"""Tensor-core (tcgen05) kernels of the learned con2prim guess against the
+CPU oracle (oracle/mlp_oracle.py), and the learned con2prim against the
+reference con2prim.
+
+Tolerances: BF16 operands (8-bit mantissa) with FP32 accumulation; forward
+outputs agree with the BF16-emulating oracle to 2e-2 of the output scale,
+gradients to 5e-2 normwise per tensor (rounding of the SiLU, exp and
+accumulation order can flip individual BF16 roundings).
+"""
+import numpy as np
+import pytest
+import torch
+
+import mlp_oracle as MO
+import parity as PT
+from astrofd_b200 import learned_c2p as LC
+
+pytestmark = pytest.mark.gpu
+
+
+def _dataset(n, seed, valid_only=False):
+    e = LC.c2p_engine()
+    X, T, U = LC.make_dataset(LC.sample_primitives(n, seed), e, valid_only=valid_only)
+    return e, X, T, U
+
+
+def _params(X, T, seed=0):
+    xmu, xsd, ymu, ysd = LC.normalisation(X, T)
+    return LC.init_params(seed, xmu, xsd, ymu, ysd)
+
+
+def test_forward_matches_oracle():
+    _, X, T, _ = _dataset(1000, 1)
+    flat = _params(X, T)
+    tr = LC.Trainer(flat)
+    Y = tr.forward(X).cpu().numpy()
+    P = LC.unpack(flat)
+    yn, *_ = MO.forward(P, X.cpu().numpy())
+    ref = yn * P["ysd"] + P["ymu"]
+    scale = np.abs(ref).max(axis=0)
+    assert np.all(np.abs(Y - ref).max(axis=0) / scale < 2e-2)
+    assert int(tr.status.item()) == 0
+
+
+@pytest.mark.parametrize("n", [128, 300, 1000])
+def test_gradients_match_oracle(n):
+    _, X, T, _ = _dataset(n, 2)
+    flat = _params(X, T, seed=3)
+    tr = LC.Trainer(flat)
+    g, loss = tr.grad_of(X, T)
+    g = g.cpu().numpy()
+    P = LC.unpack(flat)
+    loss_ref, gref = MO.loss_and_grads(P, X.cpu().numpy(), T.cpu().numpy())
+    assert abs(float(loss.item()) - loss_ref) / loss_ref < 1e-2
+    off, _ = LC.offsets()
+    for name in ("W1", "b1", "W2", "b2", "W3", "b3", "W4", "b4"):
+        o, shp = off[name]
+        got = g[o:o + int(np.prod(shp))].reshape(shp)
+        ref = gref[name]
+        err = np.abs(got - ref).max() / max(np.abs(ref).max(), 1e-30)
+        assert err < 5e-2, (name, err)
+
+
+def test_training_reduces_loss():
+    _, X, T, _ = _dataset(20000, 4)
+    tr = LC.Trainer(_params(X, T, seed=5))
+    losses = tr.train(X, T, steps=300, batch=4096, lr=3e-3, lr_end=1e-3, log_every=299)
+    assert losses[-1][1] < 0.2 * losses[0][1]
+
+
+def _perpendicular(prim):
+    """Same states with B projected perpendicular to v (v.B = 0), where the
+    reference's prim_to_cons and cons_to_prim are mutually consistent."""
+    prim = prim.copy()
+    v, b = prim[1:4], prim[5:8]
+    b -= v * (np.sum(v * b, axis=0) / np.maximum(np.sum(v * v, axis=0), 1e-300))
+    return prim
+
+
+def test_learned_c2p_matches_reference_and_beats_no_network():
+    e, X, T, U = _dataset(120000, 6, valid_only=True)
+    tr = LC.Trainer(_params(X, T, seed=7))
+    tr.train(X, T, steps=3000, batch=8192, lr=3e-3, lr_end=2e-4)
+
+    # states with v.B = 0: the residual has one physical root, so the learned
+    # path (any start, same Newton update and tolerance) lands on the
+    # reference's solution
+    _, _, Up = LC.make_dataset(_perpendicular(LC.sample_primitives(20000, 8)), e)
+    ref = e.c2p_array(Up).cpu().numpy()
+    q, st = LC.c2p_learned(e, Up, tr.params, max_polish=2)
+    rel = np.abs(q.cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-300)
+    assert st["status"] == 0 and st["cells"] == Up.shape[1]
+    assert np.all(rel[5:] == 0.0)
+    # both solutions meet |f| < 1e-10 max(1, tau), which leaves p free to
+    # ~1e-5 relative when tau >> p; beyond 1e-4 would mean another root
+    assert (rel[:5].max(axis=0) > 1e-4).mean() < 1e-2
+
+    # random v.B: the reference's p2c and c2p disagree there (its residual uses
+    # b^2 = B^2/W^2 + (S.B/Z)^2), f(Z) can have several roots and the one found
+    # depends on the start; the bulk still agrees to the Newton tolerance
+    ref = e.c2p_array(U).cpu().numpy()
+    q, st = LC.c2p_learned(e, U, tr.params, max_polish=2)
+    rel = np.abs(q.cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-300)
+    assert st["status"] == 0 and st["cells"] == U.shape[1]
+    assert (rel[:5].max(axis=0) > 1e-4).mean() < 0.05
+
+
+
+def test_network_gain_on_jet_states():
+    """What the trained network gains over the same solver without it, on the
+    states the step actually meets (cells of a magnetised-jet run): more cells
+    converge within two polish steps and fewer Newton steps are taken than from
+    the analytic start D + tau + B^2 (the reference's second Newton start)."""
+    from astrofd_b200.train_c2p_mlp import harvest_jet
+    e = LC.c2p_engine()
+    prim = harvest_jet(n=48, steps=9, per_snapshot=40000, seed=3)
+    X, T, U = LC.make_dataset(prim, e, valid_only=True)
+    Xs, Ts, _ = LC.make_dataset(LC.sample_primitives(100000, 9), e, valid_only=True)
+    half = X.shape[0] // 2
+    Xt, Tt = torch.cat([X[:half], Xs]), torch.cat([T[:half], Ts])
+    tr = LC.Trainer(_params(Xt, Tt, seed=1))
+    tr.train(Xt, Tt, steps=3000, batch=8192, lr=3e-3, lr_end=2e-4)
+    Uh = U[:, half:].contiguous()
+    _, st = LC.c2p_learned(e, Uh, tr.params, max_polish=2)
+    _, st0 = LC.c2p_learned(e, Uh, None, max_polish=2)
+    assert st["status"] == 0
+    n = Uh.shape[1]
+    assert st["learned_polish"] >= st0["learned_polish"] - 0.005 * n
+    assert st["polish_steps"] < 0.8 * st0["polish_steps"]

