@@ -316,7 +316,7 @@ template <typename RF> __device__ __forceinline__ double ldf(const void* p, size
 // DEFER: the learned con2prim runs in its own kernel, so this one only
 // writes U (the con2prim code is compiled out, which frees registers).
 template <int PHYS, typename RF, bool DEFER, bool PASSIVE>
-__global__ void __launch_bounds__(128) k_update(UpdArgs a) {
+__global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
     constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
     const size_t cell = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -486,8 +486,10 @@ __device__ __forceinline__ void c2p_features(const double* U, float* x) {
     const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
     const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
     const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
-    const double r[4] = {sqrt(S2) / D, rmax(U[4], 0.0) / D, B2 / D, SB * SB / (D * D * D)};
-    x[0] = (float)log(D);
+    const double iD = 1.0 / D;
+    const double r[4] = {sqrt(S2) * iD, rmax(U[4], 0.0) * iD, B2 * iD, SB * SB * iD * iD * iD};
+    // the features feed a float32/bfloat16 network: float32 logarithms
+    x[0] = logf((float)rmax(D, 1e-30));
 #pragma unroll
     for (int i = 0; i < 4; ++i) x[1 + i] = log1pf((float)rmin(r[i], 1e30));
 }
@@ -508,7 +510,7 @@ struct C2PArgs {
 // max_polish Newton steps of the reference's update; cells that do not meet
 // |f| < 1e-10 max(1, tau) continue with the full Newton solve from there and,
 // failing that, run the reference's complete con2prim.
-__global__ void __launch_bounds__(128) k_c2p_learned(C2PArgs a) {
+__global__ void __launch_bounds__(128, 6) k_c2p_learned(C2PArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + mlp::kInferSmem);
     uint32_t* taddr_s = reinterpret_cast<uint32_t*>(sm + mlp::kInferSmem + 8);
@@ -554,9 +556,11 @@ __global__ void __launch_bounds__(128) k_c2p_learned(C2PArgs a) {
         const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
         double Z;
         if (net) {
-            const double logW = rmax((double)(o[0] * a.net->ysd[0] + a.net->ymu[0]), 0.0);
-            const double logp = (double)(o[1] * a.net->ysd[1] + a.net->ymu[1]);
-            const double W = exp(rmin(logW, 20.0)), pg = exp(rmax(rmin(logp, 50.0), -60.0));
+            // the guess only has to start Newton: float32 exponentials
+            const float logW = fmaxf(o[0] * a.net->ysd[0] + a.net->ymu[0], 0.f);
+            const float logp = o[1] * a.net->ysd[1] + a.net->ymu[1];
+            const double W = (double)__expf(fminf(logW, 20.f));
+            const double pg = (double)__expf(fmaxf(fminf(logp, 50.f), -80.f));
             Z = rmax(D * W + gfac * pg * W * W, 1e-12);
         } else {
             Z = rmax(D + tau + B2, 1e-12);
@@ -617,13 +621,26 @@ int sm_count_cached() {
     return g_sm_count;
 }
 
+int g_c2p_blocks_per_sm = 0;
+
 cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
     const long ntiles = (a.count + mlp::TILE - 1) / mlp::TILE;
-    const long cap = 4L * sm_count_cached();
+    if (!g_c2p_blocks_per_sm) {
+        // prefer the largest shared-memory carveout so that as many 40 KB tiles
+        // are resident as registers allow (TMEM: 8 x 64 columns fit)
+        cudaFuncSetAttribute(k_c2p_learned, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_c2p_learned, mlp::TILE,
+                                                          mlp::kInferSmem + 16) != cudaSuccess)
+            nb = 0;
+        g_c2p_blocks_per_sm = nb < 4 ? 4 : (nb > 8 ? 8 : nb);
+    }
+    const long cap = (long)g_c2p_blocks_per_sm * sm_count_cached();
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     if (grid <= 0) return cudaSuccess;
     k_c2p_learned<<<grid, mlp::TILE, mlp::kInferSmem + 16, s>>>(a);
-    mark(1, s);
+    mark(3, s);
     return cudaGetLastError();
 }
 

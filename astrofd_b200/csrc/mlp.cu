@@ -237,6 +237,8 @@ cudaError_t ensure_smem_attrs() {
     cudaError_t e = cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          kTrainSmem);
     if (e != cudaSuccess) return e;
+    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     g_attr_done = true;
     return cudaSuccess;
 }

@@ -40,7 +40,8 @@ constexpr int OFF_W1 = 0;                      // [64 x 16]  bf16  2 KB
 constexpr int OFF_W2 = OFF_W1 + 64 * 16 * 2;   // [64 x 64]         8 KB
 constexpr int OFF_W3 = OFF_W2 + 64 * 64 * 2;   // [64 x 64]         8 KB
 constexpr int OFF_W4 = OFF_W3 + 64 * 64 * 2;   // [16 x 64]         2 KB
-constexpr int OFF_H0 = OFF_W4 + 16 * 64 * 2;   // [128 x 16]        4 KB
+constexpr int OFF_BIAS = OFF_W4 + 16 * 64 * 2; // b1 b2 b3 b4 f32   1 KB (read by every row)
+constexpr int OFF_H0 = OFF_BIAS + 1024;        // [128 x 16]        4 KB
 constexpr int OFF_H1 = OFF_H0 + 128 * 16 * 2;  // [128 x 64]       16 KB each
 constexpr int OFF_H2 = OFF_H1 + 128 * 64 * 2;
 constexpr int OFF_H3 = OFF_H2 + 128 * 64 * 2;
@@ -210,6 +211,9 @@ __device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P)
         float w = o < NOUT ? P->W4[o * H + i] : 0.f;
         *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W4 + elem_off(16, o, i)) = __float2bfloat16_rn(w);
     }
+    float* bs = reinterpret_cast<float*>(sm + OFF_BIAS);
+    for (int e = threadIdx.x; e < 3 * H + NOUT; e += blockDim.x)
+        bs[e] = e < H ? P->b1[e] : (e < 2 * H ? P->b2[e - H] : (e < 3 * H ? P->b3[e - 2 * H] : P->b4[e - 3 * H]));
 }
 
 // Issue D[128 x N] (+)= A[128 x K] . B for K = 16*ksteps, both operands
@@ -242,7 +246,7 @@ __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, u
         st_row8(sm + OFF_H0, 128, t, 0, v);
         st_row8(sm + OFF_H0, 128, t, 8, v + 8);
     }
-    const float* bias[3] = {P->b1, P->b2, P->b3};
+    const float* bsm = reinterpret_cast<const float*>(sm + OFF_BIAS);
     const int offW[3] = {OFF_W1, OFF_W2, OFF_W3};
     const int offDS[3] = {OFF_DS1, OFF_DS2, OFF_DS3};
     for (int l = 0; l < 4; ++l) {
@@ -271,7 +275,7 @@ __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, u
                 tmem_ld16(tmem + lane_base + cb * 16, z);
 #pragma unroll
                 for (int i = 0; i < 16; ++i) {
-                    z[i] += bias[l][cb * 16 + i];
+                    z[i] += bsm[l * H + cb * 16 + i];
                     h[i] = silu(z[i]);
                 }
                 st_row8(dst, 128, t, cb * 16, h);
@@ -287,8 +291,8 @@ __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, u
         } else {
             float y[16];
             tmem_ld16(tmem + lane_base, y);
-            out[0] = y[0] + P->b4[0];
-            out[1] = y[1] + P->b4[1];
+            out[0] = y[0] + bsm[3 * H];
+            out[1] = y[1] + bsm[3 * H + 1];
         }
     }
     return true;

@@ -184,14 +184,21 @@ template <typename R> AHD void floor_prim(const Phys<R>& P, R* q) {
     }
 }
 
-template <typename R> AHD void s_flux(const Phys<R>& P, int n, const R* q, R* F) {
-    R U[5];
-    s_p2c(P, q, U);
+// physical flux from primitives q and their conserved state U = p2c(q)
+// (the reference recomputes p2c inside flux_x/y/z, srhd_core.py:157-169; the
+// caller's U is the same value, so it is reused)
+template <typename R> AHD void s_flux_u(const Phys<R>& P, int n, const R* q, const R* U, R* F) {
     R vn = q[1 + n], p = q[4];
     F[0] = U[0] * vn;
 #pragma unroll
     for (int m = 0; m < 3; ++m) F[1 + m] = (m == n) ? U[1 + m] * vn + p : U[1 + m] * vn;
     F[4] = (U[4] + p) * vn;
+}
+
+template <typename R> AHD void s_flux(const Phys<R>& P, int n, const R* q, R* F) {
+    R U[5];
+    s_p2c(P, q, U);
+    s_flux_u(P, n, q, U, F);
 }
 
 template <typename R> AHD R contact_speed(int n, const R* UL, const R* UR, R sL, R sR, R pL,
@@ -234,8 +241,8 @@ AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
     floor_prim(P, qR);
     s_p2c(P, qL, UL);
     s_p2c(P, qR, UR);
-    s_flux(P, n, qL, FL);
-    s_flux(P, n, qR, FR);
+    s_flux_u(P, n, qL, UL, FL);
+    s_flux_u(P, n, qR, UR, FR);
     R csL = s_sound_speed(P, qL[0], qL[4]), csR = s_sound_speed(P, qR[0], qR[4]);
     eig_speeds(qL[1 + n], csL, lmL, lpL);
     eig_speeds(qR[1 + n], csR, lmR, lpR);
@@ -280,9 +287,9 @@ template <typename R> AHD void r_p2c(const Phys<R>& P, const R* qin, R* U) {
     U[5] = Bx; U[6] = By; U[7] = Bz; U[8] = qin[8];
 }
 
-template <typename R> AHD void r_flux(const Phys<R>& P, int n, const R* q, R* F) {
-    R U[9];
-    r_p2c(P, q, U);
+// physical flux from primitives q and U = p2c(q) (flux_rmhd_x/y/z,
+// rmhd_core.py:344-395, recompute p2c internally; reused here)
+template <typename R> AHD void r_flux_u(const Phys<R>& P, int n, const R* q, const R* U, R* F) {
     R v[3] = {q[1], q[2], q[3]}, B[3] = {q[5], q[6], q[7]};
     R p = q[4], psi = q[8];
     R B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
@@ -296,6 +303,12 @@ template <typename R> AHD void r_flux(const Phys<R>& P, int n, const R* q, R* F)
 #pragma unroll
     for (int m = 0; m < 3; ++m) F[5 + m] = (m == n) ? psi : v[m] * Bn - vn * B[m];
     F[8] = P.glm_ch * P.glm_ch * Bn;
+}
+
+template <typename R> AHD void r_flux(const Phys<R>& P, int n, const R* q, R* F) {
+    R U[9];
+    r_p2c(P, q, U);
+    r_flux_u(P, n, q, U, F);
 }
 
 template <typename R> AHD R r_fast_speed(const Phys<R>& P, const R* q) {
@@ -453,8 +466,8 @@ AHD void r_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
     floor_prim(P, qR);
     r_p2c(P, qL, UL);
     r_p2c(P, qR, UR);
-    r_flux(P, n, qL, FL);
-    r_flux(P, n, qR, FR);
+    r_flux_u(P, n, qL, UL, FL);
+    r_flux_u(P, n, qR, UR, FR);
     if (!GIVEN) r_speeds(P, n, qL, qR, sL, sR);
     r_riemann<RIEMANN, MUSCL_OVR>(P, n, qL, qR, UL, UR, FL, FR, sL, sR, F);
 }

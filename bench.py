@@ -313,43 +313,49 @@ def cpu_sample(args, steps, warmup):
 
 
 # ------------------------------------------------------------------ main ---
-def roofline(args, prof_ms, prof_n, prec):
-    """Dominant kernel class and its achieved HBM bandwidth (algorithmic bytes)."""
+KERNELS = {0: "k_face (float32 reconstruction + Riemann, one direction)",
+           1: "k_update (flux divergence + SSPRK3 combination)",
+           3: "k_c2p_learned (tcgen05 MLP guess + Newton polish)"}
+
+
+def roofline(args, prof_ms, prof_n, prec, learned):
+    """Dominant kernel class of the timed steps and its achieved bandwidth in
+    ALGORITHMIC bytes (the unique bytes the kernel must move) per launch."""
     peaks = {}
     pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pk):
         peaks = json.load(open(pk))
     peak = float(peaks.get("hbm_gbs", 6650.0))
     which = "measured" if "hbm_gbs" in peaks else "fallback"
-    cls = int(np.argmax(prof_ms[:2]))
+    cls = max((0, 1, 3), key=lambda c: prof_ms[c])
     nlaunch = max(int(prof_n[cls]), 1)
     avg_s = prof_ms[cls] / nlaunch / 1e3
-    n, ng, nv, nm = args.n, 3, 11, 9
+    n, ng, nv, nm, npas = args.n, 3, 11, 9, 2
     N = n + 2 * ng
     rs = 4 if prec == "mixed" else 8
     if cls == 0:
-        # face pass in one direction: each face reads one new primitive column
-        # (nm float64) and writes its flux (nm values); faces ~ n^3 (+1 plane)
-        units = (n + 1) * n * n
-        per_unit = nm * 8 + nm * rs
-        name = "k_face (reconstruction + Riemann, one direction)"
+        # one direction: every face reads one new column of nm float64
+        # primitives and writes its nm fluxes
+        units, per_unit = (n + 1) * n * n, nm * 8 + nm * rs
+    elif cls == 1:
+        # every cell: 3 flux buffers, pr0 (nv), pr_k psi + passives, U_{k-1}
+        # (stages 2-3), U_k, the next primitives (all nv, or the non-main ones
+        # when the learned con2prim writes the main ones)
+        u_in = 2.0 / 3.0 * nm * 8
+        u_out = nm * 8 if learned else 2.0 / 3.0 * nm * 8
+        dst = (nv - nm) * 8 if learned else nv * 8
+        units, per_unit = N ** 3, 3 * nm * rs + nv * 8 + (npas + 1) * 8 + u_in + u_out + dst
     else:
-        # stage update over all N^3 cells: 3 face fluxes, pr0 and pr_k (nv
-        # float64 each), U_k-1 and U_k (nm float64), writes next primitives
-        units = N ** 3
-        per_unit = 3 * nm * rs + 2 * nv * 8 + 2 * nm * 8 + nv * 8
-        name = "k_update (divergence + SSPRK + con2prim)"
+        units, per_unit = N ** 3, 2 * nm * 8  # U in, primitives out
     achieved = units * per_unit / avg_s / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
-        t = json.load(open(tf)).get(f"{prec}:{cls}")
-        if t:
-            traffic = t
-    return {"bound": "hbm", "kernel": name, "achieved": round(achieved, 1),
+        traffic = json.load(open(tf)).get(f"{prec}:{cls}:{n}")
+    return {"bound": "hbm", "kernel": KERNELS[cls], "achieved": round(achieved, 1),
             "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": traffic, "peak_source": which,
-            "bytes_per_launch": units * per_unit, "avg_launch_ms": round(avg_s * 1e3, 4),
+            "bytes_per_launch": int(units * per_unit), "avg_launch_ms": round(avg_s * 1e3, 4),
             "class_share": round(float(prof_ms[cls] / max(prof_ms.sum(), 1e-30)), 3)}
 
 
@@ -468,9 +474,11 @@ def main():
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
-        "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed"),
+        "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed", learned),
         "kernel_ms_per_step": {"face": round(mixed["prof_ms"][0] / args.steps, 3),
-                               "update": round(mixed["prof_ms"][1] / args.steps, 3)},
+                               "update": round(mixed["prof_ms"][1] / args.steps, 3),
+                               "c2p_learned": round(mixed["prof_ms"][3] / args.steps, 3),
+                               "other": round(mixed["prof_ms"][2] / args.steps, 3)},
         "finite": mixed["finite"],
         "c2p": mixed["c2p"],
     }

@@ -154,7 +154,8 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in,
 
 /* Per-kernel-class device time of one step, from CUDA events recorded after
  * every launch.  Classes: 0 face-flux passes, 1 stage update (divergence, RK,
- * con2prim), 2 other (ghost fills, reductions, sources), 3 reserved. */
+ * and con2prim unless learned), 2 other (ghost fills, reductions, sources),
+ * 3 learned con2prim. */
 typedef struct AstroKernelTimes {
     double ms[4];
     int32_t launches[4];
