@@ -136,6 +136,9 @@ int validate(const AstroParams* p, const AstroGrid* g) {
     if (p->physics == ASTRO_SRHD && (g->nv >= 15 || (p->n_passive > 0 && p->passive_offset != 5)))
         return ASTRO_E_UNSUPPORTED;
     if (g->nx < 8 || g->ny < 8 || g->nz < 8) return ASTRO_E_SHAPE;
+    // cell indices are 32-bit in the kernels; 2^31 cells of even 5 float64
+    // variables exceed the device memory
+    if ((double)g->nx * g->ny * g->nz >= 2147483648.0) return ASTRO_E_SHAPE;
     if (!(g->dx > 0) || !(g->dy > 0) || !(g->dz > 0)) return ASTRO_E_INVALID;
     return ASTRO_OK;
 }
@@ -313,22 +316,106 @@ template <typename RF> __device__ __forceinline__ double ldf(const void* p, size
     return (double)__ldg((const RF*)p + i);
 }
 
-// DEFER: the learned con2prim runs in its own kernel, so this one only
-// writes U (the con2prim code is compiled out, which frees registers).
+// asynchronous global -> shared copies of one 4- or 8-byte value (cp.async);
+// the issuing thread reads its own copies after cp_async_wait_all
+template <typename T> __device__ __forceinline__ void cp_async(T* s, const T* g) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte values");
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+    if constexpr (sizeof(T) == 4)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// Staged update (DEFER): shared memory per thread holds the 6*NM face fluxes
+// of its cell, then the float64 values it reads once: q0[NM], U_k[NM], psi
+// and the three B components of the stage input, passives t0[np], t_k[np].
+constexpr int kUpdateBlock = 128;
+inline size_t update_smem_bytes(int nm, size_t rf_bytes, int np) {
+    return ((size_t)6 * nm * rf_bytes + (size_t)(2 * nm + 4 + 2 * np) * 8) * kUpdateBlock;
+}
+
+// DEFER: the learned con2prim runs in its own kernel, so this one only writes
+// U (the con2prim code is compiled out, which frees registers), and every
+// value a cell reads once is first copied to shared memory with cp.async, all
+// of a thread's copies in flight together, so that the pass is bound by HBM
+// bandwidth rather than by the latency of one dependent load after another.
 template <int PHYS, typename RF, bool DEFER, bool PASSIVE>
-__global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
+__global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k_update(UpdArgs a) {
     constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
-    const size_t nc = (size_t)a.nx * a.ny * a.nz;
-    const size_t cell = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    constexpr bool STAGE = DEFER;
+    constexpr int T = kUpdateBlock;
+    extern __shared__ __align__(16) unsigned char ush[];
+    const unsigned nc32 = (unsigned)a.nx * (unsigned)a.ny * (unsigned)a.nz;
+    const size_t nc = nc32;
+    const unsigned cell32 = blockIdx.x * T + threadIdx.x;
+    const size_t cell = cell32;
+    const int tid = threadIdx.x;
+    RF* sF = reinterpret_cast<RF*>(ush);
+    double* sD = reinterpret_cast<double*>(ush + (size_t)6 * NM * sizeof(RF) * T);
+    const int np = a.p.n_passive, po = a.p.passive_offset;
+    // float64 item slots
+    const int I_U = NM, I_PSI = 2 * NM, I_B = 2 * NM + 1, I_T0 = 2 * NM + 4, I_TK = 2 * NM + 4 + np;
     C2PCount cnt;
-    if (cell < nc) {
-        const int k = (int)(cell % a.nz);
-        const int j = (int)((cell / a.nz) % a.ny);
-        const int i = (int)(cell / ((size_t)a.nz * a.ny));
-        const bool in = i >= a.b.lo && i < a.b.hi[0] && j >= a.b.lo && j < a.b.hi[1] &&
-                        k >= a.b.lo && k < a.b.hi[2];
+    if (cell32 < nc32) {
+        const unsigned k = cell32 % (unsigned)a.nz;
+        const unsigned r32 = cell32 / (unsigned)a.nz;
+        const unsigned j = r32 % (unsigned)a.ny;
+        const unsigned i = r32 / (unsigned)a.ny;
+        const bool in = (int)i >= a.b.lo && (int)i < a.b.hi[0] && (int)j >= a.b.lo &&
+                        (int)j < a.b.hi[1] && (int)k >= a.b.lo && (int)k < a.b.hi[2];
         const long st[3] = {(long)a.ny * a.nz, (long)a.nz, 1L};
-        const int np = a.p.n_passive, po = a.p.passive_offset;
+        int nres = 0;
+        if (PHYS == ASTRO_RMHD && a.p.resistive && a.p.resistivity > 0.0) {
+            // conservative mode applies eta*Laplacian(B) exactly once for
+            // every reconstruction (the reference adds it twice for PPM and
+            // not at all for WENO, rmhd_core.py:1414-1435,1440-1557)
+            nres = a.p.flux_mode == ASTRO_FLUX_CONSERVATIVE
+                       ? 1
+                       : (a.p.recon == ASTRO_RECON_MUSCL ? 1 : (a.p.recon == ASTRO_RECON_PPM ? 2 : 0));
+        }
+        if constexpr (STAGE) {
+            if (in) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+#pragma unroll
+                    for (int v = 0; v < NM; ++v) {
+                        const size_t o = (size_t)v * nc + cell;
+                        const RF* lo = (const RF*)(d == 0 ? a.FxL : a.F[d]);
+                        cp_async(&sF[((d * NM + v) * 2 + 1) * T + tid], (const RF*)a.F[d] + o + st[d]);
+                        cp_async(&sF[((d * NM + v) * 2 + 0) * T + tid], lo + o);
+                    }
+                if (PHYS == ASTRO_RMHD) {
+                    cp_async(&sD[I_PSI * T + tid], a.prk + 8 * nc + cell);
+                    if (nres)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                            cp_async(&sD[(I_B + c) * T + tid], a.prk + (size_t)(5 + c) * nc + cell);
+                }
+            }
+            if (!a.rhs_only) {
+#pragma unroll
+                for (int v = 0; v < NM; ++v) {
+                    cp_async(&sD[v * T + tid], a.pr0 + (size_t)v * nc + cell);
+                    if (a.stage) cp_async(&sD[(I_U + v) * T + tid], a.U + (size_t)v * nc + cell);
+                }
+                for (int t = 0; t < np; ++t) {
+                    const size_t o = (size_t)(po + t) * nc + cell;
+                    cp_async(&sD[(I_T0 + t) * T + tid], a.pr0 + o);
+                    if (a.stage) cp_async(&sD[(I_TK + t) * T + tid], a.prk + o);
+                }
+            }
+            cp_async_wait_all();
+        }
+        auto flux = [&](int d, int v, int hi) -> double {
+            if constexpr (STAGE) return (double)sF[((d * NM + v) * 2 + hi) * T + tid];
+            const size_t o = (size_t)v * nc + cell;
+            if (hi) return ldf<RF>(a.F[d], o + st[d]);
+            return ldf<RF>(d == 0 ? a.FxL : a.F[d], o);
+        };
         double rhs[NM];
         double rp[kMaxPassive];
 #pragma unroll
@@ -337,24 +424,16 @@ __global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
         if (in) {
 #pragma unroll
             for (int v = 0; v < NM; ++v) {
-                const size_t o = (size_t)v * nc + cell;
                 double r = 0.0;
-                r -= (ldf<RF>(a.F[0], o + st[0]) - ldf<RF>(a.FxL, o)) / a.dd[0];
-                r -= (ldf<RF>(a.F[1], o + st[1]) - ldf<RF>(a.F[1], o)) / a.dd[1];
-                r -= (ldf<RF>(a.F[2], o + st[2]) - ldf<RF>(a.F[2], o)) / a.dd[2];
+                r -= (flux(0, v, 1) - flux(0, v, 0)) / a.dd[0];
+                r -= (flux(1, v, 1) - flux(1, v, 0)) / a.dd[1];
+                r -= (flux(2, v, 1) - flux(2, v, 0)) / a.dd[2];
                 rhs[v] = r;
             }
             if (PHYS == ASTRO_RMHD) {
                 const double* q = a.prk;
-                rhs[8] -= a.p.glm_cp * a.p.glm_cp * q[8 * nc + cell];
-                int nres = (a.p.resistive && a.p.resistivity > 0.0)
-                               ? (a.p.recon == ASTRO_RECON_MUSCL ? 1 : (a.p.recon == ASTRO_RECON_PPM ? 2 : 0))
-                               : 0;
-                // conservative mode applies eta*Laplacian(B) exactly once for
-                // every reconstruction (the reference adds it twice for PPM and
-                // not at all for WENO, rmhd_core.py:1414-1435,1440-1557)
-                if (a.p.flux_mode == ASTRO_FLUX_CONSERVATIVE)
-                    nres = (a.p.resistive && a.p.resistivity > 0.0) ? 1 : 0;
+                const double psi = STAGE ? sD[I_PSI * T + tid] : q[8 * nc + cell];
+                rhs[8] -= a.p.glm_cp * a.p.glm_cp * psi;
                 for (int rep = 0; rep < nres; ++rep) {
                     const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
                     const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
@@ -362,9 +441,10 @@ __global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
 #pragma unroll
                     for (int c = 5; c < 8; ++c) {
                         const double* B = q + (size_t)c * nc + cell;
-                        double lap = (B[st[0]] - 2.0 * B[0] + B[-st[0]]) * ix2 +
-                                     (B[st[1]] - 2.0 * B[0] + B[-st[1]]) * iy2 +
-                                     (B[st[2]] - 2.0 * B[0] + B[-st[2]]) * iz2;
+                        const double b0 = STAGE ? sD[(I_B + c - 5) * T + tid] : B[0];
+                        double lap = (B[st[0]] - 2.0 * b0 + B[-st[0]]) * ix2 +
+                                     (B[st[1]] - 2.0 * b0 + B[-st[1]]) * iy2 +
+                                     (B[st[2]] - 2.0 * b0 + B[-st[2]]) * iz2;
                         rhs[c] += a.p.resistivity * lap;
                     }
                 }
@@ -410,7 +490,7 @@ __global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
             const Phys<double> P = Phys<double>::from(a.p);
             double q0[NM], U0[NM], Un[NM], q[NM];
 #pragma unroll
-            for (int v = 0; v < NM; ++v) q0[v] = a.pr0[(size_t)v * nc + cell];
+            for (int v = 0; v < NM; ++v) q0[v] = STAGE ? sD[v * T + tid] : a.pr0[(size_t)v * nc + cell];
             if (PHYS == ASTRO_SRHD) s_p2c(P, q0, U0);
             else r_p2c(P, q0, U0);
             const double dt = a.dt;
@@ -420,7 +500,7 @@ __global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
                 double un;
                 if (a.stage == 0) un = __dadd_rn(u0, __dmul_rn(dt, r));
                 else {
-                    const double uk = a.U[(size_t)v * nc + cell];
+                    const double uk = STAGE ? sD[(I_U + v) * T + tid] : a.U[(size_t)v * nc + cell];
                     if (a.nstages == 2)
                         un = __dmul_rn(0.5, __dadd_rn(__dadd_rn(u0, uk), __dmul_rn(dt, r)));
                     else if (a.stage == 1)
@@ -446,10 +526,10 @@ __global__ void __launch_bounds__(128, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
                 const int t = v - po;
                 if (np > 0 && t >= 0 && t < np) {
                     const size_t o = (size_t)v * nc + cell;
-                    const double t0 = a.pr0[o], r = rp[t];
+                    const double t0 = STAGE ? sD[(I_T0 + t) * T + tid] : a.pr0[o], r = rp[t];
                     if (a.stage == 0) out = __dadd_rn(t0, __dmul_rn(dt, r));
                     else {
-                        const double tk = a.prk[o];
+                        const double tk = STAGE ? sD[(I_TK + t) * T + tid] : a.prk[o];
                         if (a.nstages == 2)
                             out = __dmul_rn(0.5, __dadd_rn(__dadd_rn(t0, tk), __dmul_rn(dt, r)));
                         else if (a.stage == 1)
@@ -626,15 +706,26 @@ int g_c2p_blocks_per_sm = 0;
 cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
     const long ntiles = (a.count + mlp::TILE - 1) / mlp::TILE;
     if (!g_c2p_blocks_per_sm) {
-        // prefer the largest shared-memory carveout so that as many 40 KB tiles
-        // are resident as registers allow (TMEM: 8 x 64 columns fit)
+        // prefer the largest shared-memory carveout and size the persistent
+        // grid by what is resident per SM: shared memory (one 42 KB tile
+        // each), registers, and TMEM (8 blocks x 64 columns)
         cudaFuncSetAttribute(k_c2p_learned, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_c2p_learned, mlp::TILE,
-                                                          mlp::kInferSmem + 16) != cudaSuccess)
-            nb = 0;
-        g_c2p_blocks_per_sm = nb < 4 ? 4 : (nb > 8 ? 8 : nb);
+        int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 65536;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+        cudaFuncAttributes fa;
+        int nb = 4;
+        if (cudaFuncGetAttributes(&fa, k_c2p_learned) == cudaSuccess && smem_sm > 0) {
+            const int per_block = mlp::kInferSmem + 16 + (int)fa.sharedSizeBytes + reserved;
+            const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
+            const int by_smem = smem_sm / per_block;
+            const int by_regs = regs_sm / (regs_warp > 0 ? regs_warp * (mlp::TILE / 32) : 1);
+            nb = by_smem < by_regs ? by_smem : by_regs;
+        }
+        g_c2p_blocks_per_sm = nb < 1 ? 1 : (nb > 8 ? 8 : nb);
     }
     const long cap = (long)g_c2p_blocks_per_sm * sm_count_cached();
     const int grid = (int)(ntiles < cap ? ntiles : cap);
@@ -698,19 +789,41 @@ cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// one update launch; the staged (DEFER) variants take dynamic shared memory,
+// whose per-kernel limit is raised once to the largest size they can ask for
+template <int PH, typename RF, bool DEF, bool PAS>
+void launch_update_t(const UpdArgs& a, dim3 grd, dim3 blk, cudaStream_t s) {
+    constexpr int nm = PH == ASTRO_SRHD ? 5 : 9;
+    size_t smem = 0;
+    if (DEF) {
+        static bool attr[64] = {};
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev < 0 || dev >= 64 || !attr[dev]) {
+            cudaFuncSetAttribute(k_update<PH, RF, DEF, PAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)update_smem_bytes(nm, sizeof(RF), kMaxPassive));
+            cudaFuncSetAttribute(k_update<PH, RF, DEF, PAS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+            if (dev >= 0 && dev < 64) attr[dev] = true;
+        }
+        smem = update_smem_bytes(nm, sizeof(RF), a.p.n_passive);
+    }
+    k_update<PH, RF, DEF, PAS><<<grd, blk, smem, s>>>(a);
+}
+
 cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
-    const dim3 blk(128), grd((unsigned)((nc + 127) / 128));
+    const dim3 blk(kUpdateBlock), grd((unsigned)((nc + kUpdateBlock - 1) / kUpdateBlock));
     const bool mixed = a.p.precision == ASTRO_PREC_MIXED;
     const bool pas = passive_fluxes(a.p);
 #define UPD(PH, DEF)                                                               \
     do {                                                                           \
         if (pas) {                                                                 \
-            if (mixed) k_update<PH, float, DEF, true><<<grd, blk, 0, s>>>(a);      \
-            else k_update<PH, double, DEF, true><<<grd, blk, 0, s>>>(a);           \
+            if (mixed) launch_update_t<PH, float, DEF, true>(a, grd, blk, s);      \
+            else launch_update_t<PH, double, DEF, true>(a, grd, blk, s);           \
         } else {                                                                   \
-            if (mixed) k_update<PH, float, DEF, false><<<grd, blk, 0, s>>>(a);     \
-            else k_update<PH, double, DEF, false><<<grd, blk, 0, s>>>(a);          \
+            if (mixed) launch_update_t<PH, float, DEF, false>(a, grd, blk, s);     \
+            else launch_update_t<PH, double, DEF, false>(a, grd, blk, s);          \
         }                                                                          \
     } while (0)
     if (a.p.physics == ASTRO_SRHD) UPD(ASTRO_SRHD, false);

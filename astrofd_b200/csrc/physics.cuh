@@ -33,6 +33,37 @@ template <typename R> AHD R rmin(R a, R b) { return a < b ? a : b; }
 template <typename R> AHD R rsqrt_(R x) { return sqrt(x); }
 template <typename R> AHD R rabs(R x) { return x < R(0) ? -x : x; }
 
+// The float32 face path takes one approximate reciprocal per shared
+// denominator (rcp.approx.ftz.f32, one MUFU operation, relative error about
+// one ulp) and rsqrt.approx.ftz.f32 for 1/sqrt, where a division compiles to
+// a reciprocal plus range fix-ups; the float64 path keeps the reference's
+// IEEE divisions and square roots exactly as written.
+template <typename R> AHD R rcp_(R x) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 4) {
+        float y;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+        return y;
+    }
+#endif
+    return R(1) / x;
+}
+template <typename R> AHD R rsq_(R x) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 4) {
+        float y;
+        asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+        return y;
+    }
+#endif
+    return R(1) / sqrt(x);
+}
+// a / b: float32 as a * rcp(b), float64 as the IEEE quotient
+template <typename R> AHD R qdiv(R a, R b) {
+    if constexpr (sizeof(R) == 4) return a * rcp_(b);
+    else return a / b;
+}
+
 // Physical parameters in the arithmetic type of the caller.
 template <typename R> struct Phys {
     R gamma, srhd_gamma, p_max, v_max, glm_ch, glm_cp;
@@ -88,15 +119,24 @@ template <typename R> AHD R weno5(R a, R b, R c, R d, R e) {
     R IS0 = R(13.0 / 12.0) * (t0 * t0) + R(0.25) * (u0 * u0);
     R IS1 = R(13.0 / 12.0) * (t1 * t1) + R(0.25) * (u1 * u1);
     R IS2 = R(13.0 / 12.0) * (t2 * t2) + R(0.25) * (u2 * u2);
-    R a0 = R(0.1) / ((eps + IS0) * (eps + IS0));
-    R a1 = R(0.6) / ((eps + IS1) * (eps + IS1));
-    R a2 = R(0.3) / ((eps + IS2) * (eps + IS2));
-    R s = a0 + a1 + a2;
-    R w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
     R p0 = R(1.0 / 3.0) * a - R(7.0 / 6.0) * b + R(11.0 / 6.0) * c;
     R p1 = R(-1.0 / 6.0) * b + R(5.0 / 6.0) * c + R(1.0 / 3.0) * d;
     R p2 = R(1.0 / 3.0) * c + R(5.0 / 6.0) * d - R(1.0 / 6.0) * e;
-    return w0 * p0 + w1 * p1 + w2 * p2;
+    if constexpr (sizeof(R) == 4) {
+        // four reciprocals instead of six divisions; a weight whose
+        // (eps + IS)^2 overflows goes to 0 as in the quotient form
+        const R a0 = R(0.1) * rcp_((eps + IS0) * (eps + IS0));
+        const R a1 = R(0.6) * rcp_((eps + IS1) * (eps + IS1));
+        const R a2 = R(0.3) * rcp_((eps + IS2) * (eps + IS2));
+        return (a0 * p0 + a1 * p1 + a2 * p2) * rcp_(a0 + a1 + a2);
+    } else {
+        R a0 = R(0.1) / ((eps + IS0) * (eps + IS0));
+        R a1 = R(0.6) / ((eps + IS1) * (eps + IS1));
+        R a2 = R(0.3) / ((eps + IS2) * (eps + IS2));
+        R s = a0 + a1 + a2;
+        R w0 = a0 / s, w1 = a1 / s, w2 = a2 / s;
+        return w0 * p0 + w1 * p1 + w2 * p2;
+    }
 }
 
 // Left/right states at the face between cell c-1 and c from a stencil
@@ -129,15 +169,29 @@ AHD void hlle(const R* UL, const R* UR, const R* FL, const R* FR, R sL, R sR, R*
     if (sL >= R(0)) { for (int v = 0; v < N; ++v) out[v] = FL[v]; return; }
     if (sR <= R(0)) { for (int v = 0; v < N; ++v) out[v] = FR[v]; return; }
     R inv = sR - sL + C<R>::small;
+    if constexpr (sizeof(R) == 4) {
+        const R ri = rcp_(inv);
 #pragma unroll
-    for (int v = 0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) / inv;
+        for (int v = 0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) * ri;
+    } else {
+#pragma unroll
+        for (int v = 0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) / inv;
+    }
 }
 
 template <typename R> AHD void eig_speeds(R vn, R cs, R& lm, R& lp) {
     R dp = R(1) + vn * cs, dm = R(1) - vn * cs;
     if (dp == R(0)) dp = C<R>::small;
     if (dm == R(0)) dm = C<R>::small;
-    R p = (vn + cs) / dp, m = (vn - cs) / dm;
+    R p, m;
+    if constexpr (sizeof(R) == 4) {
+        const R r = rcp_(dp * dm);
+        p = (vn + cs) * dm * r;
+        m = (vn - cs) * dp * r;
+    } else {
+        p = (vn + cs) / dp;
+        m = (vn - cs) / dm;
+    }
     if (p > R(1)) p = R(1);
     if (p < R(-1)) p = R(-1);
     if (m > R(1)) m = R(1);
@@ -151,8 +205,8 @@ template <typename R> AHD void s_p2c(const Phys<R>& P, const R* q, R* U) {
     R rho = q[0], vx = q[1], vy = q[2], vz = q[3], p = q[4];
     R v2 = vx * vx + vy * vy + vz * vz;
     if (v2 >= R(1)) v2 = R(1) - R(1e-14);
-    R W = R(1) / rsqrt_(R(1) - v2);
-    R h = R(1) + gamma / (gamma - R(1)) * p / rmax(rho, C<R>::small);
+    R W = sizeof(R) == 4 ? rsq_(R(1) - v2) : R(1) / rsqrt_(R(1) - v2);
+    R h = R(1) + qdiv(gamma / (gamma - R(1)) * p, rmax(rho, C<R>::small));
     R w = rho * h;
     U[0] = rho * W;
     R wW2 = w * W * W;
@@ -164,9 +218,9 @@ template <typename R> AHD void s_p2c(const Phys<R>& P, const R* q, R* U) {
 
 template <typename R> AHD R s_sound_speed(const Phys<R>& P, R rho, R p) {
     const R gamma = P.srhd_gamma;
-    R h = R(1) + gamma / (gamma - R(1)) * p / rmax(rho, C<R>::small);
+    R h = R(1) + qdiv(gamma / (gamma - R(1)) * p, rmax(rho, C<R>::small));
     R w = rho * h;
-    R cs2 = gamma * p / rmax(w, C<R>::small);
+    R cs2 = qdiv(gamma * p, rmax(w, C<R>::small));
     if (cs2 < R(0)) cs2 = R(0);
     if (cs2 > R(1) - R(1e-14)) cs2 = R(1) - R(1e-14);
     return rsqrt_(cs2);
@@ -204,7 +258,7 @@ template <typename R> AHD void s_flux(const Phys<R>& P, int n, const R* q, R* F)
 template <typename R> AHD R contact_speed(int n, const R* UL, const R* UR, R sL, R sR, R pL,
                                           R pR, R vL, R vR) {
     R denom = (UL[0] * (sL - vL) - UR[0] * (sR - vR)) + C<R>::small;
-    return (pR - pL + UL[1 + n] * (sL - vL) - UR[1 + n] * (sR - vR)) / denom;
+    return qdiv(pR - pL + UL[1 + n] * (sL - vL) - UR[1 + n] * (sR - vR), denom);
 }
 
 // HLLC for SRHD / the hydro block of RMHD "hlld"
@@ -215,20 +269,30 @@ AHD void hllc5(int n, const R* UL, const R* UR, const R* FL, const R* FR, R sL, 
     if (sR <= R(0)) { for (int v = 0; v < 5; ++v) out[v] = FR[v]; return; }
     R DL = UL[0], DR = UR[0];
     R denom = (DL * (sL - vL) - DR * (sR - vR)) + C<R>::small;
-    R sM = (pR - pL + UL[1 + n] * (sL - vL) - UR[1 + n] * (sR - vR)) / denom;
+    R sM = qdiv(pR - pL + UL[1 + n] * (sL - vL) - UR[1 + n] * (sR - vR), denom);
     R pStar = R(0.5) * (pL + pR + DL * (sL - vL) * (sM - vL) + DR * (sR - vR) * (sM - vR));
     const bool left = sM >= R(0);
     const R* U = left ? UL : UR;
     const R* F = left ? FL : FR;
     R s = left ? sL : sR, pK = left ? pL : pR, vK = left ? vL : vR;
     R den = s - sM + C<R>::small;
-    R fac = (s - vK) / den;
+    R fac, dpx, dex;
+    if constexpr (sizeof(R) == 4) {
+        const R rd = rcp_(den);
+        fac = (s - vK) * rd;
+        dpx = (pStar - pK) * rd;
+        dex = (pStar * sM - pK * vK) * rd;
+    } else {
+        fac = (s - vK) / den;
+        dpx = (pStar - pK) / den;
+        dex = (pStar * sM - pK * vK) / den;
+    }
     R Ust[5];
     Ust[0] = U[0] * fac;
 #pragma unroll
     for (int m = 0; m < 3; ++m)
-        Ust[1 + m] = (m == n) ? U[1 + m] * fac + (pStar - pK) / den : U[1 + m] * fac;
-    Ust[4] = U[4] * fac + (pStar * sM - pK * vK) / den;
+        Ust[1 + m] = (m == n) ? U[1 + m] * fac + dpx : U[1 + m] * fac;
+    Ust[4] = U[4] * fac + dex;
 #pragma unroll
     for (int v = 0; v < 5; ++v) out[v] = F[v] + s * (Ust[v] - U[v]);
 }
@@ -268,13 +332,22 @@ template <typename R> AHD void r_p2c(const Phys<R>& P, const R* qin, R* U) {
     if (p < C<R>::small) p = C<R>::small;
     if (p > P.p_max) p = P.p_max;
     R B2 = Bx * Bx + By * By + Bz * Bz;
-    R W = R(1) / rsqrt_(R(1) - (vx * vx + vy * vy + vz * vz));
-    R h = R(1) + gamma / (gamma - R(1)) * p / rmax(rho, C<R>::small);
+    R W, bx, by, bz;
+    R h = R(1) + qdiv(gamma / (gamma - R(1)) * p, rmax(rho, C<R>::small));
     R rhoh = rho * h;
     R vb = vx * Bx + vy * By + vz * Bz;
+    if constexpr (sizeof(R) == 4) {
+        const R om = R(1) - (vx * vx + vy * vy + vz * vz);
+        W = rsq_(om);
+        const R iW = om * W;  // sqrt(1 - v^2)
+        const R b0 = W * vb;
+        bx = (Bx + b0 * vx) * iW; by = (By + b0 * vy) * iW; bz = (Bz + b0 * vz) * iW;
+    } else {
+        W = R(1) / rsqrt_(R(1) - (vx * vx + vy * vy + vz * vz));
+        const R b0 = W * vb;  // divisions kept as in the reference
+        bx = (Bx + b0 * vx) / W; by = (By + b0 * vy) / W; bz = (Bz + b0 * vz) / W;
+    }
     R b0 = W * vb;
-    R iW = W;  // divisions kept as in the reference
-    R bx = (Bx + b0 * vx) / iW, by = (By + b0 * vy) / iW, bz = (Bz + b0 * vz) / iW;
     R b2 = (bx * bx + by * by + bz * bz) - b0 * b0;
     R rhohW2 = rhoh * W * W;
     R wtot = rhohW2 + B2;
@@ -317,20 +390,29 @@ template <typename R> AHD R r_fast_speed(const Phys<R>& P, const R* q) {
     R Bx = q[5], By = q[6], Bz = q[7];
     R v2 = vx * vx + vy * vy + vz * vz;
     if (v2 >= P.v_max * P.v_max) v2 = P.v_max * P.v_max - R(1e-14);
-    R W = R(1) / rsqrt_(R(1) - v2);
     if (rho < C<R>::small) rho = C<R>::small;
     if (p < C<R>::small) p = C<R>::small;
     if (p > P.p_max) p = P.p_max;
-    R h = R(1) + G / (G - R(1)) * p / rmax(rho, C<R>::small);
+    R h = R(1) + qdiv(G / (G - R(1)) * p, rmax(rho, C<R>::small));
     R rhoh = rho * h;
     R vb = vx * Bx + vy * By + vz * Bz;
+    R W, bx, by, bz;
+    if constexpr (sizeof(R) == 4) {
+        W = rsq_(R(1) - v2);
+        const R iW = (R(1) - v2) * W;
+        const R b0 = W * vb;
+        bx = (Bx + b0 * vx) * iW; by = (By + b0 * vy) * iW; bz = (Bz + b0 * vz) * iW;
+    } else {
+        W = R(1) / rsqrt_(R(1) - v2);
+        const R b0 = W * vb;
+        bx = (Bx + b0 * vx) / W; by = (By + b0 * vy) / W; bz = (Bz + b0 * vz) / W;
+    }
     R b0 = W * vb;
-    R bx = (Bx + b0 * vx) / W, by = (By + b0 * vy) / W, bz = (Bz + b0 * vz) / W;
     R b2 = (bx * bx + by * by + bz * bz) - b0 * b0;
-    R cs2 = G * p / rmax(rhoh, C<R>::small);
+    R cs2 = qdiv(G * p, rmax(rhoh, C<R>::small));
     if (cs2 < R(0)) cs2 = R(0);
     if (cs2 > R(1) - R(1e-14)) cs2 = R(1) - R(1e-14);
-    R ca2 = b2 / rmax(rhoh + b2, C<R>::small);
+    R ca2 = qdiv(b2, rmax(rhoh + b2, C<R>::small));
     if (ca2 < R(0)) ca2 = R(0);
     if (ca2 > R(1) - R(1e-14)) ca2 = R(1) - R(1e-14);
     R a = cs2 + ca2 - cs2 * ca2;
