@@ -62,7 +62,7 @@ class AstroC2PStats(C.Structure):
 
 
 class AstroKernelTimes(C.Structure):
-    _fields_ = [("ms", C.c_double * 4), ("launches", C.c_int32 * 4)]
+    _fields_ = [("ms", C.c_double * 5), ("launches", C.c_int32 * 5)]
 
 
 # every symbol include/astrofd.h declares, with its ctypes prototype

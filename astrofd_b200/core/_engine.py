@@ -138,7 +138,7 @@ class Engine:
                                          float(dt), int(rk_order), rt.ptr(w), nb, rt.ptr(stats),
                                          rt.stream_handle(pr.device), C.byref(times)),
                    "astro_step_profiled")
-        return out, [times.ms[i] for i in range(4)], [times.launches[i] for i in range(4)]
+        return out, [times.ms[i] for i in range(5)], [times.launches[i] for i in range(5)]
 
     def _stats_buffer(self, device):
         if self.stats is None or self.stats.device != torch.device(device):

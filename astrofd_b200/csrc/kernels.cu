@@ -77,7 +77,7 @@ __host__ Bounds bounds_of(const AstroParams& p, const AstroGrid& g) {
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
-    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, total;
+    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, c2pfb, total;
 };
 
 inline bool carried_mode(const AstroParams& p) {
@@ -98,6 +98,18 @@ inline size_t fix_capacity(const AstroGrid& g) {
     return nc / 16 + 1024;
 }
 
+// learned con2prim: cells whose Newton polish fails are listed (cell, Z) and
+// solved by a second kernel in dense warps; cells beyond the capacity are
+// solved inline
+struct C2PFallback {
+    unsigned cell, mode;  // mode 0: Newton from Z, then the full con2prim; 1: full con2prim
+    double Z;
+};
+inline size_t c2p_fb_capacity(const AstroGrid& g) {
+    const size_t nc = (size_t)g.nx * g.ny * g.nz;
+    return nc / 32 + 1024;
+}
+
 Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
     Layout L;
     const size_t nc = (size_t)g.nx * g.ny * g.nz;
@@ -114,6 +126,9 @@ Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
     L.Sz = carried_mode(p) ? take(2 * nc * rs) : 0;
     // float32 passes: counter + list of faces to recompute in float64
     L.fix = p.precision == ASTRO_PREC_MIXED ? take(256 + fix_capacity(g) * sizeof(unsigned)) : 0;
+    L.c2pfb = (with_state && p.c2p_guess == ASTRO_GUESS_LEARNED)
+                  ? take(256 + c2p_fb_capacity(g) * sizeof(C2PFallback))
+                  : 0;
     L.total = o;
     return L;
 }
@@ -583,7 +598,18 @@ struct C2PArgs {
     AstroC2PStats* stats;
     int* status;
     int max_polish;
+    unsigned* fb_count = nullptr;  // null: every cell is solved in k_c2p_learned
+    C2PFallback* fb_list = nullptr;
+    unsigned fb_cap = 0;
 };
+
+__device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell, unsigned mode, double Z) {
+    if (!a.fb_list) return false;
+    const unsigned slot = atomicAdd(a.fb_count, 1u);
+    if (slot >= a.fb_cap) return false;
+    a.fb_list[slot] = C2PFallback{(unsigned)cell, mode, Z};
+    return true;
+}
 
 // Learned con2prim: per 128-cell tile the MLP (tcgen05, BF16, FP32 accumulate)
 // predicts (log W, log p); Z = D W + Gamma/(Gamma-1) p W^2 starts at most
@@ -652,9 +678,13 @@ __global__ void __launch_bounds__(128, 6) k_c2p_learned(C2PArgs a) {
             ++n_polish;
             polish_steps += steps;
             done = r_prims_from_Z_checked(P, Z, U, q);
+            if (!done && c2p_defer(a, cell, 1u, Z)) continue;
         } else {
             ++n_fallback;
             polish_steps += a.max_polish;
+            // the long solves go to k_c2p_fallback, so that they do not hold
+            // up the 31 other cells of this warp
+            if (c2p_defer(a, cell, 0u, Z)) continue;
             if (isfinite(Z) && r_newton(P, Z, 50, D, tau, B2, SB, S2)) {
                 cnt.newton++;
                 done = r_prims_from_Z_checked(P, Z, U, q);
@@ -674,6 +704,40 @@ __global__ void __launch_bounds__(128, 6) k_c2p_learned(C2PArgs a) {
         if (n_polish) atomicAdd(&a.stats->learned_polish, (unsigned long long)n_polish);
         if (n_fallback) atomicAdd(&a.stats->learned_fallback, (unsigned long long)n_fallback);
         if (polish_steps) atomicAdd(&a.stats->polish_steps, (unsigned long long)polish_steps);
+        if (cnt.newton) atomicAdd(&a.stats->newton, (unsigned long long)cnt.newton);
+        if (cnt.bisect) atomicAdd(&a.stats->bisection, (unsigned long long)cnt.bisect);
+        if (cnt.hydro_fallback) atomicAdd(&a.stats->hydro_fallback, (unsigned long long)cnt.hydro_fallback);
+    }
+}
+
+// The cells k_c2p_learned listed: Newton from the polished Z (mode 0) and,
+// failing that, the reference's complete con2prim, one cell per thread.
+__global__ void __launch_bounds__(128) k_c2p_fallback(C2PArgs a) {
+    const unsigned n = min(*a.fb_count, a.fb_cap);
+    const Phys<double> P = Phys<double>::from(a.p);
+    C2PCount cnt;
+    for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        const C2PFallback f = a.fb_list[e];
+        const size_t cell = f.cell;
+        double U[9], q[9];
+#pragma unroll
+        for (int v = 0; v < 9; ++v) U[v] = a.U[(size_t)v * a.count + cell];
+        bool done = false;
+        double Z = f.Z;
+        if (f.mode == 0u && isfinite(Z)) {
+            const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
+            const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
+            const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
+            if (r_newton(P, Z, 50, U[0], U[4], B2, SB, S2)) {
+                cnt.newton++;
+                done = r_prims_from_Z_checked(P, Z, U, q);
+            }
+        }
+        if (!done) r_c2p(P, U, q, cnt);
+#pragma unroll
+        for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
+    }
+    if (a.stats) {
         if (cnt.newton) atomicAdd(&a.stats->newton, (unsigned long long)cnt.newton);
         if (cnt.bisect) atomicAdd(&a.stats->bisection, (unsigned long long)cnt.bisect);
         if (cnt.hydro_fallback) atomicAdd(&a.stats->hydro_fallback, (unsigned long long)cnt.hydro_fallback);
@@ -730,8 +794,14 @@ cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
     const long cap = (long)g_c2p_blocks_per_sm * sm_count_cached();
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     if (grid <= 0) return cudaSuccess;
+    if (a.fb_list && cudaMemsetAsync(a.fb_count, 0, sizeof(unsigned), s) != cudaSuccess)
+        return cudaGetLastError();
     k_c2p_learned<<<grid, mlp::TILE, mlp::kInferSmem + 16, s>>>(a);
     mark(3, s);
+    if (a.fb_list) {
+        k_c2p_fallback<<<sm_count_cached() * 4, 128, 0, s>>>(a);
+        mark(4, s);
+    }
     return cudaGetLastError();
 }
 
@@ -1225,6 +1295,9 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
             c.count = (long)g->nx * g->ny * g->nz;
             c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
             c.status = nullptr; c.max_polish = 2;
+            c.fb_count = (unsigned*)(w + L.c2pfb);
+            c.fb_list = (C2PFallback*)(w + L.c2pfb + 256);
+            c.fb_cap = (unsigned)c2p_fb_capacity(*g);
             e = launch_c2p_learned(c, s);
             if (e != cudaSuccess) return ASTRO_E_CUDA;
         }
@@ -1254,7 +1327,7 @@ int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* 
         for (int i = 0; i < P.n; ++i) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, P.ev[i], P.ev[i + 1]);
-            const int k = P.kind[i] < 4 ? P.kind[i] : 3;
+            const int k = P.kind[i] < 5 ? P.kind[i] : 2;
             times->ms[k] += ms;
             times->launches[k] += 1;
         }

@@ -206,8 +206,8 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     L = _lib.load()
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    prof_ms = np.zeros(4)
-    prof_n = np.zeros(4, dtype=np.int64)
+    prof_ms = np.zeros(5)
+    prof_n = np.zeros(5, dtype=np.int64)
     barrier(world)
     torch.cuda.synchronize()
     l0 = L.astro_launch_count()
@@ -478,6 +478,7 @@ def main():
         "kernel_ms_per_step": {"face": round(mixed["prof_ms"][0] / args.steps, 3),
                                "update": round(mixed["prof_ms"][1] / args.steps, 3),
                                "c2p_learned": round(mixed["prof_ms"][3] / args.steps, 3),
+                               "c2p_fallback": round(mixed["prof_ms"][4] / args.steps, 3),
                                "other": round(mixed["prof_ms"][2] / args.steps, 3)},
         "finite": mixed["finite"],
         "c2p": mixed["c2p"],

@@ -155,10 +155,10 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in,
 /* Per-kernel-class device time of one step, from CUDA events recorded after
  * every launch.  Classes: 0 face-flux passes, 1 stage update (divergence, RK,
  * and con2prim unless learned), 2 other (ghost fills, reductions, sources),
- * 3 learned con2prim. */
+ * 3 learned con2prim, 4 learned con2prim's fallback solves. */
 typedef struct AstroKernelTimes {
-    double ms[4];
-    int32_t launches[4];
+    double ms[5];
+    int32_t launches[5];
 } AstroKernelTimes;
 
 /* astro_step with per-launch event timing filled into *times.  Synchronises
