@@ -344,6 +344,13 @@ template <typename T> __device__ __forceinline__ void cp_async(T* s, const T* g)
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+// wait until at most one committed group of this thread is in flight
+__device__ __forceinline__ void cp_async_wait_but_one() {
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+}
 
 // Staged update (DEFER): shared memory per thread holds the 6*NM face fluxes
 // of its cell, then the float64 values it reads once: q0[NM], U_k[NM], psi
@@ -411,6 +418,8 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                             cp_async(&sD[(I_B + c) * T + tid], a.prk + (size_t)(5 + c) * nc + cell);
                 }
             }
+            // two groups: the divergence runs while the RK operands arrive
+            cp_async_commit();
             if (!a.rhs_only) {
 #pragma unroll
                 for (int v = 0; v < NM; ++v) {
@@ -423,7 +432,8 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                     if (a.stage) cp_async(&sD[(I_TK + t) * T + tid], a.prk + o);
                 }
             }
-            cp_async_wait_all();
+            cp_async_commit();
+            cp_async_wait_but_one();
         }
         auto flux = [&](int d, int v, int hi) -> double {
             if constexpr (STAGE) return (double)sF[((d * NM + v) * 2 + hi) * T + tid];
@@ -437,13 +447,27 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
         for (int v = 0; v < NM; ++v) rhs[v] = 0.0;
         for (int t = 0; t < np; ++t) rp[t] = 0.0;
         if (in) {
+            if constexpr (sizeof(RF) == 4) {
+                // float32 fluxes: multiply by 1/dx (the float64 path divides
+                // as the reference does)
+                const double i0 = 1.0 / a.dd[0], i1 = 1.0 / a.dd[1], i2 = 1.0 / a.dd[2];
 #pragma unroll
-            for (int v = 0; v < NM; ++v) {
-                double r = 0.0;
-                r -= (flux(0, v, 1) - flux(0, v, 0)) / a.dd[0];
-                r -= (flux(1, v, 1) - flux(1, v, 0)) / a.dd[1];
-                r -= (flux(2, v, 1) - flux(2, v, 0)) / a.dd[2];
-                rhs[v] = r;
+                for (int v = 0; v < NM; ++v) {
+                    double r = 0.0;
+                    r -= (flux(0, v, 1) - flux(0, v, 0)) * i0;
+                    r -= (flux(1, v, 1) - flux(1, v, 0)) * i1;
+                    r -= (flux(2, v, 1) - flux(2, v, 0)) * i2;
+                    rhs[v] = r;
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < NM; ++v) {
+                    double r = 0.0;
+                    r -= (flux(0, v, 1) - flux(0, v, 0)) / a.dd[0];
+                    r -= (flux(1, v, 1) - flux(1, v, 0)) / a.dd[1];
+                    r -= (flux(2, v, 1) - flux(2, v, 0)) / a.dd[2];
+                    rhs[v] = r;
+                }
             }
             if (PHYS == ASTRO_RMHD) {
                 const double* q = a.prk;
@@ -497,6 +521,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                 }
             }
         }
+        if constexpr (STAGE) cp_async_wait_all();
         if (a.rhs_only) {
 #pragma unroll
             for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = rhs[v];
@@ -616,7 +641,7 @@ __device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell, unsigned 
 // max_polish Newton steps of the reference's update; cells that do not meet
 // |f| < 1e-10 max(1, tau) continue with the full Newton solve from there and,
 // failing that, run the reference's complete con2prim.
-__global__ void __launch_bounds__(128, 6) k_c2p_learned(C2PArgs a) {
+__global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + mlp::kInferSmem);
     uint32_t* taddr_s = reinterpret_cast<uint32_t*>(sm + mlp::kInferSmem + 8);

@@ -198,6 +198,21 @@ __device__ __forceinline__ float silu_grad(float z) {
     return s * (1.0f + z * (1.0f - s));
 }
 
+// SiLU of 16 accumulator columns after adding their biases, two columns per
+// packed float32x2 instruction (sm_100 FADD2/FMUL2/FFMA2)
+__device__ __forceinline__ void bias_silu16(const float* z, const float* bias, float* h) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float2 b = *reinterpret_cast<const float2*>(bias + 2 * i);
+        const float2 zz = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]), b);
+        const float2 hh = __fmul2_rn(zz, make_float2(0.5f, 0.5f));
+        const float2 tt = make_float2(tanh_approx(hh.x), tanh_approx(hh.y));
+        const float2 ss = __ffma2_rn(hh, tt, hh);
+        h[2 * i] = hh.x < -8.f ? 0.f : ss.x;
+        h[2 * i + 1] = hh.y < -8.f ? 0.f : ss.y;
+    }
+}
+
 // write 8 consecutive columns [c0, c0+8) of row r as bf16 (16-byte store)
 __device__ __forceinline__ void st_row8(unsigned char* base, int R, int r, int c0, const float* v) {
     __nv_bfloat162 p[4];
@@ -287,10 +302,14 @@ __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, u
             for (int cb = 0; cb < 4; ++cb) {
                 float z[16], h[16];
                 tmem_ld16(tmem + lane_base + cb * 16, z);
+                if (TRAIN) {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) z[i] += bsm[l * H + cb * 16 + i];
+                    for (int i = 0; i < 16; ++i) z[i] += bsm[l * H + cb * 16 + i];
 #pragma unroll
-                for (int i = 0; i < 16; ++i) h[i] = silu(z[i]);
+                    for (int i = 0; i < 16; ++i) h[i] = silu(z[i]);
+                } else {
+                    bias_silu16(z, bsm + l * H + cb * 16, h);
+                }
                 st_row8(dst, 128, t, cb * 16, h);
                 st_row8(dst, 128, t, cb * 16 + 8, h + 8);
                 if (TRAIN) {

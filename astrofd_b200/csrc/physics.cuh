@@ -139,6 +139,41 @@ template <typename R> AHD R weno5(R a, R b, R c, R d, R e) {
     }
 }
 
+#ifdef __CUDA_ARCH__
+// Both WENO5 face values of a float32 stencil s[0..5] at once: lane x is the
+// left-biased value weno5(s0..s4), lane y the right-biased weno5(s5..s1), the
+// same formula on mirrored stencils, so every add/multiply is one packed
+// float32x2 instruction (FADD2/FMUL2/FFMA2) and only the reciprocals are
+// scalar.
+__device__ __forceinline__ float2 weno5_pair(const float* s) {
+    const float2 A = make_float2(s[0], s[5]), B = make_float2(s[1], s[4]);
+    const float2 Cc = make_float2(s[2], s[3]), D = make_float2(s[3], s[2]);
+    const float2 E = make_float2(s[4], s[1]);
+    auto k2 = [](float c) { return make_float2(c, c); };
+    const float2 m2 = k2(-2.f);
+    const float2 t0 = __fadd2_rn(__ffma2_rn(B, m2, A), Cc);
+    const float2 u0 = __ffma2_rn(Cc, k2(3.f), __ffma2_rn(B, k2(-4.f), A));
+    const float2 t1 = __fadd2_rn(__ffma2_rn(Cc, m2, B), D);
+    const float2 u1 = __fadd2_rn(B, __fmul2_rn(D, k2(-1.f)));
+    const float2 t2 = __fadd2_rn(__ffma2_rn(D, m2, Cc), E);
+    const float2 u2 = __fadd2_rn(__ffma2_rn(D, k2(-4.f), __fmul2_rn(Cc, k2(3.f))), E);
+    const float2 c13 = k2(13.f / 12.f), q = k2(0.25f), eps = k2(1e-12f);
+    const float2 w0 = __fadd2_rn(__ffma2_rn(__fmul2_rn(t0, c13), t0, __fmul2_rn(__fmul2_rn(u0, q), u0)), eps);
+    const float2 w1 = __fadd2_rn(__ffma2_rn(__fmul2_rn(t1, c13), t1, __fmul2_rn(__fmul2_rn(u1, q), u1)), eps);
+    const float2 w2 = __fadd2_rn(__ffma2_rn(__fmul2_rn(t2, c13), t2, __fmul2_rn(__fmul2_rn(u2, q), u2)), eps);
+    const float2 v0 = __fmul2_rn(w0, w0), v1 = __fmul2_rn(w1, w1), v2 = __fmul2_rn(w2, w2);
+    const float2 a0 = __fmul2_rn(make_float2(rcp_(v0.x), rcp_(v0.y)), k2(0.1f));
+    const float2 a1 = __fmul2_rn(make_float2(rcp_(v1.x), rcp_(v1.y)), k2(0.6f));
+    const float2 a2 = __fmul2_rn(make_float2(rcp_(v2.x), rcp_(v2.y)), k2(0.3f));
+    const float2 p0 = __ffma2_rn(Cc, k2(11.f / 6.f), __ffma2_rn(B, k2(-7.f / 6.f), __fmul2_rn(A, k2(1.f / 3.f))));
+    const float2 p1 = __ffma2_rn(D, k2(1.f / 3.f), __ffma2_rn(Cc, k2(5.f / 6.f), __fmul2_rn(B, k2(-1.f / 6.f))));
+    const float2 p2 = __ffma2_rn(E, k2(-1.f / 6.f), __ffma2_rn(D, k2(5.f / 6.f), __fmul2_rn(Cc, k2(1.f / 3.f))));
+    const float2 num = __ffma2_rn(a2, p2, __ffma2_rn(a1, p1, __fmul2_rn(a0, p0)));
+    const float2 den = __fadd2_rn(__fadd2_rn(a0, a1), a2);
+    return __fmul2_rn(num, make_float2(rcp_(den.x), rcp_(den.y)));
+}
+#endif
+
 // Left/right states at the face between cell c-1 and c from a stencil
 // a[0..5] = q(c-3) .. q(c+2).  MUSCL uses a[1..4].
 template <int RECON, typename R> AHD void recon_face(const R* a, int lim, R& qL, R& qR) {
@@ -153,6 +188,14 @@ template <int RECON, typename R> AHD void recon_face(const R* a, int lim, R& qL,
         ppm(a[1], a[2], a[3], a[4], a[5], l1, r1);
         qL = r0; qR = l1;
     } else {
+#ifdef __CUDA_ARCH__
+        if constexpr (sizeof(R) == 4) {
+            const float2 lr = weno5_pair(a);
+            qL = lr.x;
+            qR = lr.y;
+            return;
+        }
+#endif
         qL = weno5(a[0], a[1], a[2], a[3], a[4]);
         qR = weno5(a[5], a[4], a[3], a[2], a[1]);
     }

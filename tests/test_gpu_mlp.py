@@ -106,15 +106,35 @@ def test_learned_c2p_matches_reference_and_beats_no_network():
 
 
 
-def test_network_gain_on_jet_states():
-    """What the trained network gains over the same solver without it, on the
-    states the step actually meets (cells of a magnetised-jet run): more cells
-    converge within two polish steps and fewer Newton steps are taken than from
-    the analytic start D + tau + B^2 (the reference's second Newton start)."""
+def _jet_states(e):
     from astrofd_b200.train_c2p_mlp import harvest_jet
-    e = LC.c2p_engine()
     prim = harvest_jet(n=48, steps=9, per_snapshot=40000, seed=3)
-    X, T, U = LC.make_dataset(prim, e, valid_only=True)
+    return LC.make_dataset(prim, e, valid_only=True)
+
+
+def test_network_gain_on_jet_states():
+    """What the shipped network (astrofd_b200/data/c2p_mlp.npz, trained on
+    states of a 128^3 jet run) gains over the same solver without it, on states
+    of a different (48^3, other seed) jet run: as many cells converge within
+    two polish steps and far fewer Newton steps are taken than from the
+    analytic start D + tau + B^2 (the reference's second Newton start)."""
+    e = LC.c2p_engine()
+    _, _, U = _jet_states(e)
+    params = torch.as_tensor(LC.load(), dtype=torch.float32).cuda()
+    _, st = LC.c2p_learned(e, U, params, max_polish=2)
+    _, st0 = LC.c2p_learned(e, U, None, max_polish=2)
+    assert st["status"] == 0
+    n = U.shape[1]
+    assert st["learned_polish"] >= st0["learned_polish"] - 0.005 * n
+    assert st["polish_steps"] < 0.7 * st0["polish_steps"], (st, st0)
+
+
+def test_training_on_jet_states_gains():
+    """A network trained here (3000 Adam steps of the tensor-core kernels on
+    half of the harvested jet states plus sampler states) already saves Newton
+    steps on the other half."""
+    e = LC.c2p_engine()
+    X, T, U = _jet_states(e)
     Xs, Ts, _ = LC.make_dataset(LC.sample_primitives(100000, 9), e, valid_only=True)
     half = X.shape[0] // 2
     Xt, Tt = torch.cat([X[:half], Xs]), torch.cat([T[:half], Ts])
@@ -126,4 +146,4 @@ def test_network_gain_on_jet_states():
     assert st["status"] == 0
     n = Uh.shape[1]
     assert st["learned_polish"] >= st0["learned_polish"] - 0.005 * n
-    assert st["polish_steps"] < 0.8 * st0["polish_steps"]
+    assert st["polish_steps"] < 0.95 * st0["polish_steps"], (st, st0)
