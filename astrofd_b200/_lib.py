@@ -99,8 +99,9 @@ PROTOS = {
     "astro_mlp_train_grad": (C.c_int, [_VP, _DP, _DP, C.c_int64, _DP, _DP, _VP, _VP]),
     "astro_mlp_adam": (C.c_int, [_VP, _DP, _DP, _DP, C.c_float, C.c_float, C.c_float,
                                  C.c_float, C.c_int, _VP]),
+    "astro_c2p_learned_workspace_bytes": (C.c_size_t, [C.c_int64]),
     "astro_c2p_learned": (C.c_int, [C.POINTER(AstroParams), _DP, _DP, C.c_int64, C.c_int,
-                                    _VP, _VP, _VP]),
+                                    _VP, C.c_size_t, _VP, _VP, _VP]),
     "astro_cooling_heating": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, C.c_double,
                                         C.c_double, C.c_double, C.c_double, _VP]),
     "astro_two_temperature": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, C.c_double,

@@ -77,7 +77,7 @@ __host__ Bounds bounds_of(const AstroParams& p, const AstroGrid& g) {
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
-    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, c2pfb, total;
+    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, c2pfb, prf, total;
 };
 
 inline bool carried_mode(const AstroParams& p) {
@@ -98,13 +98,8 @@ inline size_t fix_capacity(const AstroGrid& g) {
     return nc / 16 + 1024;
 }
 
-// learned con2prim: cells whose Newton polish fails are listed (cell, Z) and
-// solved by a second kernel in dense warps; cells beyond the capacity are
-// solved inline
-struct C2PFallback {
-    unsigned cell, mode;  // mode 0: Newton from Z, then the full con2prim; 1: full con2prim
-    double Z;
-};
+// learned con2prim: cells whose Newton polish fails are listed and solved by
+// a second kernel in dense warps; cells beyond the capacity are solved inline
 inline size_t c2p_fb_capacity(const AstroGrid& g) {
     const size_t nc = (size_t)g.nx * g.ny * g.nz;
     return nc / 32 + 1024;
@@ -126,8 +121,10 @@ Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
     L.Sz = carried_mode(p) ? take(2 * nc * rs) : 0;
     // float32 passes: counter + list of faces to recompute in float64
     L.fix = p.precision == ASTRO_PREC_MIXED ? take(256 + fix_capacity(g) * sizeof(unsigned)) : 0;
+    // float32 copy of the nm primitives the float32 face passes read
+    L.prf = p.precision == ASTRO_PREC_MIXED ? take((size_t)nm * nc * sizeof(float)) : 0;
     L.c2pfb = (with_state && p.c2p_guess == ASTRO_GUESS_LEARNED)
-                  ? take(256 + c2p_fb_capacity(g) * sizeof(C2PFallback))
+                  ? take(256 + c2p_fb_capacity(g) * sizeof(unsigned))
                   : 0;
     L.total = o;
     return L;
@@ -161,6 +158,7 @@ int validate(const AstroParams* p, const AstroGrid* g) {
 // ------------------------------------------------------------ face pass ---
 struct FaceArgs {
     const double* pr;
+    const float* prf;    // float32 copy of the nm primitives (float32 passes)
     int nx, ny, nz;
     int dir;
     int org[3], ext[3];  // first cell and extents of the face block
@@ -193,9 +191,17 @@ __device__ __forceinline__ bool face_at(const FaceArgs& a, int i, int j, int k) 
 #pragma unroll
     for (int v = 0; v < NM; ++v) {
         R st[6];
-        const double* base = a.pr + (size_t)v * nc + cell;
+        if constexpr (sizeof(R) == 4) {
+            // the float32 copy: one conversion per cell and stage instead of
+            // one per stencil use
+            const float* base = a.prf + (size_t)v * nc + cell;
 #pragma unroll
-        for (int o = o0; o <= o1; ++o) st[o + 3] = (R)__ldg(base + o * stride);
+            for (int o = o0; o <= o1; ++o) st[o + 3] = __ldg(base + o * stride);
+        } else {
+            const double* base = a.pr + (size_t)v * nc + cell;
+#pragma unroll
+            for (int o = o0; o <= o1; ++o) st[o + 3] = (R)__ldg(base + o * stride);
+        }
         recon_face<RECON>(st, a.p.limiter, qL[v], qR[v]);
     }
     R F[NM];
@@ -285,6 +291,7 @@ struct UpdArgs {
     const double* prk;   // this stage's input primitives
     double* U;           // U_{k-1} in, U_k out (may be null for rhs-only)
     double* dst;         // next primitives (stage mode) or rhs (rhs mode)
+    float* dstf;         // optional float32 copy of the next nm primitives
     const void* F[3];
     const void* FxL;     // x-low-face fluxes (== F[0] unless carried mode)
     const void* aux[3];
@@ -560,6 +567,9 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                 else r_c2p(P, Un, q, cnt);
 #pragma unroll
                 for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = q[v];
+                if (a.dstf)
+#pragma unroll
+                    for (int v = 0; v < NM; ++v) a.dstf[(size_t)v * nc + cell] = (float)q[v];
             }
             for (int v = NM; v < a.nv; ++v) {
                 double out = 0.0;
@@ -617,6 +627,7 @@ __device__ __forceinline__ void c2p_features(const double* U, float* x) {
 struct C2PArgs {
     const double* U;   // [9][count]
     double* q;         // [>=9][count]: rows 0..8 written
+    float* qf = nullptr;  // optional float32 copy of rows 0..8 (next stage's faces)
     long count;
     AstroParams p;
     const mlp::Params* net;
@@ -624,23 +635,23 @@ struct C2PArgs {
     int* status;
     int max_polish;
     unsigned* fb_count = nullptr;  // null: every cell is solved in k_c2p_learned
-    C2PFallback* fb_list = nullptr;
+    unsigned* fb_list = nullptr;   // cell indices
     unsigned fb_cap = 0;
 };
 
-__device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell, unsigned mode, double Z) {
+__device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell) {
     if (!a.fb_list) return false;
     const unsigned slot = atomicAdd(a.fb_count, 1u);
     if (slot >= a.fb_cap) return false;
-    a.fb_list[slot] = C2PFallback{(unsigned)cell, mode, Z};
+    a.fb_list[slot] = (unsigned)cell;
     return true;
 }
 
 // Learned con2prim: per 128-cell tile the MLP (tcgen05, BF16, FP32 accumulate)
 // predicts (log W, log p); Z = D W + Gamma/(Gamma-1) p W^2 starts at most
 // max_polish Newton steps of the reference's update; cells that do not meet
-// |f| < 1e-10 max(1, tau) continue with the full Newton solve from there and,
-// failing that, run the reference's complete con2prim.
+// |f| < 1e-10 max(1, tau) then (or whose primitives from Z are invalid) get
+// the reference's complete con2prim, so their result is the reference's.
 __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + mlp::kInferSmem);
@@ -703,21 +714,20 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
             ++n_polish;
             polish_steps += steps;
             done = r_prims_from_Z_checked(P, Z, U, q);
-            if (!done && c2p_defer(a, cell, 1u, Z)) continue;
+            if (!done && c2p_defer(a, cell)) continue;
         } else {
             ++n_fallback;
             polish_steps += a.max_polish;
-            // the long solves go to k_c2p_fallback, so that they do not hold
-            // up the 31 other cells of this warp
-            if (c2p_defer(a, cell, 0u, Z)) continue;
-            if (isfinite(Z) && r_newton(P, Z, 50, D, tau, B2, SB, S2)) {
-                cnt.newton++;
-                done = r_prims_from_Z_checked(P, Z, U, q);
-            }
+            // the reference's complete con2prim, in k_c2p_fallback so that the
+            // long solves do not hold up the 31 other cells of this warp
+            if (c2p_defer(a, cell)) continue;
         }
         if (!done) r_c2p(P, U, q, cnt);
 #pragma unroll
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
+        if (a.qf)
+#pragma unroll
+            for (int v = 0; v < 9; ++v) a.qf[(size_t)v * a.count + cell] = (float)q[v];
     }
     if (net) {
         mlp::tc_fence_before();
@@ -735,32 +745,23 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     }
 }
 
-// The cells k_c2p_learned listed: Newton from the polished Z (mode 0) and,
-// failing that, the reference's complete con2prim, one cell per thread.
+// The cells k_c2p_learned listed: the reference's complete con2prim, one cell
+// per thread.
 __global__ void __launch_bounds__(128) k_c2p_fallback(C2PArgs a) {
     const unsigned n = min(*a.fb_count, a.fb_cap);
     const Phys<double> P = Phys<double>::from(a.p);
     C2PCount cnt;
     for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        const C2PFallback f = a.fb_list[e];
-        const size_t cell = f.cell;
+        const size_t cell = a.fb_list[e];
         double U[9], q[9];
 #pragma unroll
         for (int v = 0; v < 9; ++v) U[v] = a.U[(size_t)v * a.count + cell];
-        bool done = false;
-        double Z = f.Z;
-        if (f.mode == 0u && isfinite(Z)) {
-            const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
-            const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
-            const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
-            if (r_newton(P, Z, 50, U[0], U[4], B2, SB, S2)) {
-                cnt.newton++;
-                done = r_prims_from_Z_checked(P, Z, U, q);
-            }
-        }
-        if (!done) r_c2p(P, U, q, cnt);
+        r_c2p(P, U, q, cnt);
 #pragma unroll
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
+        if (a.qf)
+#pragma unroll
+            for (int v = 0; v < 9; ++v) a.qf[(size_t)v * a.count + cell] = (float)q[v];
     }
     if (a.stats) {
         if (cnt.newton) atomicAdd(&a.stats->newton, (unsigned long long)cnt.newton);
@@ -828,6 +829,14 @@ cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
         mark(4, s);
     }
     return cudaGetLastError();
+}
+
+// float32 copy of the first nm primitive rows (stage inputs that no
+// con2prim kernel of this library produced)
+__global__ void k_prim_f32(const double* __restrict__ pr, float* __restrict__ prf, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        prf[i] = (float)pr[i];
 }
 
 // ------------------------------------------------------------- dispatch ---
@@ -930,16 +939,24 @@ cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
 }
 
 // All face passes of one stage: z (with speeds in carried mode), x, carried x, y.
+// prf_ready: the float32 copy of pr was written by the kernel that produced pr
 cudaError_t face_passes(const AstroParams& p, const AstroGrid& g, const Bounds& b,
-                        const double* pr, char* work, const Layout& L, cudaStream_t s) {
+                        const double* pr, char* work, const Layout& L, cudaStream_t s,
+                        bool prf_ready = false) {
     const bool carried = carried_mode(p);
     const bool mixed = p.precision == ASTRO_PREC_MIXED;
     const int order[3] = {2, 0, 1};
+    float* prf = mixed ? (float*)(work + L.prf) : nullptr;
+    if (mixed && !prf_ready) {
+        const size_t n = (size_t)(p.physics == ASTRO_SRHD ? 5 : 9) * g.nx * g.ny * g.nz;
+        k_prim_f32<<<sm_count_cached() * 8, 256, 0, s>>>(pr, prf, n);
+        mark(0, s);
+    }
     for (int oi = 0; oi < 3; ++oi) {
         const int d = order[oi];
         FaceArgs a;
         memset(&a, 0, sizeof(a));
-        a.pr = pr; a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.dir = d; a.b = b; a.p = p;
+        a.pr = pr; a.prf = prf; a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.dir = d; a.b = b; a.p = p;
         for (int e = 0; e < 3; ++e) {
             a.org[e] = b.lo;
             a.ext[e] = b.hi[e] - b.lo + (e == d ? 1 : 0);
@@ -1304,12 +1321,17 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
     const int nst = rk_order;
     const double* cur = pr_in;
     double* bufs[2] = {(double*)(w + L.prA), (double*)(w + L.prB)};
+    const bool mixed = p->precision == ASTRO_PREC_MIXED;
     for (int st = 0; st < nst; ++st) {
-        cudaError_t e = face_passes(*p, *g, b, cur, w, L, s);
+        // stage 0 converts its input to the float32 copy; later stages get the
+        // copy from the kernel that produced their primitives
+        cudaError_t e = face_passes(*p, *g, b, cur, w, L, s, st > 0);
         if (e != cudaSuccess) return ASTRO_E_CUDA;
         double* dst = (st == nst - 1) ? pr_out : bufs[st % 2];
+        float* dstf = (mixed && st < nst - 1) ? (float*)(w + L.prf) : nullptr;
         UpdArgs u = update_args(*p, *g, b, w, L);
         u.pr0 = pr_in; u.prk = cur; u.U = (double*)(w + L.U); u.dst = dst;
+        u.dstf = learned ? nullptr : dstf;
         u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
         u.defer_c2p = learned ? 1 : 0;
         e = launch_update(u, s);
@@ -1321,8 +1343,9 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
             c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
             c.status = nullptr; c.max_polish = 2;
             c.fb_count = (unsigned*)(w + L.c2pfb);
-            c.fb_list = (C2PFallback*)(w + L.c2pfb + 256);
+            c.fb_list = (unsigned*)(w + L.c2pfb + 256);
             c.fb_cap = (unsigned)c2p_fb_capacity(*g);
+            c.qf = dstf;
             e = launch_c2p_learned(c, s);
             if (e != cudaSuccess) return ASTRO_E_CUDA;
         }
@@ -1457,8 +1480,14 @@ int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, dou
     return cuda_status(cudaGetLastError());
 }
 
+size_t astro_c2p_learned_workspace_bytes(int64_t count) {
+    if (count < 0) return 0;
+    return 256 + ((size_t)count / 32 + 1024) * sizeof(unsigned);
+}
+
 int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
-                      int max_polish, AstroC2PStats* stats, int* status, void* stream) {
+                      int max_polish, void* work, size_t work_bytes, AstroC2PStats* stats,
+                      int* status, void* stream) {
     if (!p || !cons || !prim || count < 0 || p->physics != ASTRO_RMHD) return ASTRO_E_INVALID;
     if (max_polish < 0 || max_polish > 50) return ASTRO_E_INVALID;
     if (count == 0) return ASTRO_OK;
@@ -1466,6 +1495,14 @@ int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, in
     c.U = cons; c.q = prim; c.count = count; c.p = *p;
     c.net = (const mlp::Params*)p->mlp; c.stats = stats; c.status = status;
     c.max_polish = max_polish;
+    if (work) {
+        // fallback list: cell indices are 32-bit
+        if (work_bytes < astro_c2p_learned_workspace_bytes(count)) return ASTRO_E_WORKSPACE;
+        if (count >= (int64_t)UINT32_MAX) return ASTRO_E_SHAPE;
+        c.fb_count = (unsigned*)work;
+        c.fb_list = (unsigned*)((char*)work + 256);
+        c.fb_cap = (unsigned)((size_t)count / 32 + 1024);
+    }
     return cuda_status(launch_c2p_learned(c, (cudaStream_t)stream));
 }
 

@@ -204,9 +204,10 @@ class Trainer:
         return Y
 
 
-def c2p_learned(engine, U, params, max_polish=2):
+def c2p_learned(engine, U, params, max_polish=2, listed=True):
     """Batch con2prim with the learned guess (params=None: Z = D + tau + B^2
-    start).  Returns (primitives [9,n], stats dict)."""
+    start).  listed: solve the states whose polish fails in a second kernel
+    (else inline).  Returns (primitives [9,n], stats dict)."""
     L = _lib.load()
     p = _lib.AstroParams()
     C.memmove(C.byref(p), C.byref(engine.p), C.sizeof(p))
@@ -214,8 +215,11 @@ def c2p_learned(engine, U, params, max_polish=2):
     out = torch.empty_like(U)
     stats = torch.zeros(8, dtype=torch.int64, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    nb = L.astro_c2p_learned_workspace_bytes(U.shape[1]) if listed else 0
+    w = rt.workspace(nb, U.device) if listed else None
     _lib.check(L.astro_c2p_learned(C.byref(p), rt.ptr(U), rt.ptr(out), U.shape[1], int(max_polish),
-                                   rt.ptr(stats), rt.ptr(status), rt.stream_handle()),
+                                   rt.ptr(w) if listed else None, nb, rt.ptr(stats),
+                                   rt.ptr(status), rt.stream_handle()),
                "astro_c2p_learned")
     names = [f for f, _ in _lib.AstroC2PStats._fields_]
     st = dict(zip(names, stats.cpu().tolist()))

@@ -57,6 +57,11 @@ def parse():
                     help="learned con2prim weights (.npz); default: the packaged network")
     ap.add_argument("--no-learned", action="store_true",
                     help="headline arm without the learned con2prim guess")
+    ap.add_argument("--c2p-batch", type=int, default=0, metavar="STATES",
+                    help="learned con2prim on a batch of sampled states (2^24 for the "
+                         "batch config) against the full float64 Newton, then exit")
+    ap.add_argument("--c2p-jet", action="store_true",
+                    help="with --c2p-batch: states of a 128^3 jet run instead of the sampler")
     ap.add_argument("--validate-steps", type=int, default=0,
                     help="instead of timing: run this many steps of mixed+learned, plain "
                          "float64 and float64 with a 1e-12 density perturbation and report "
@@ -413,12 +418,22 @@ def validate(args):
     per, _ = run("fp64", False, perturb=1e-12)
     i = slice(3, -3)
 
-    def l1(a, b):
-        return float(((a[0, i, i, i] - b[0, i, i, i]).abs().mean() / b[0, i, i, i].abs().mean()).item())
+    def fields(q):
+        q = q[:, i, i, i]
+        return {"rho": q[0], "p": q[4],
+                "W": 1.0 / torch.sqrt(1.0 - (q[1] ** 2 + q[2] ** 2 + q[3] ** 2))}
 
+    def norms(a, b):
+        fa, fb = fields(a), fields(b)
+        return {k: {"l1": float(((fa[k] - fb[k]).abs().mean() / fb[k].abs().mean()).item()),
+                    "linf": float(((fa[k] - fb[k]).abs().max() / fb[k].abs().max()).item())}
+                for k in fb}
+
+    nm, npr = norms(mix, ref), norms(per, ref)
     out = {"validate_steps": K, "grid": n, "flux_mode": args.flux_mode,
-           "rho_l1_mixed_learned_vs_fp64": l1(mix, ref),
-           "rho_l1_fp64_perturbed_1e-12_vs_fp64": l1(per, ref),
+           "rho_l1_mixed_learned_vs_fp64": nm["rho"]["l1"],
+           "rho_l1_fp64_perturbed_1e-12_vs_fp64": npr["rho"]["l1"],
+           "mixed_learned_vs_fp64": nm, "fp64_perturbed_1e-12_vs_fp64": npr,
            "c2p_fp64": st_ref, "c2p_mixed_learned": st_mix}
     # mass: one conservative step of the same state with nothing crossing the
     # faces of the update region (ambient at rest there) keeps sum(D) to round-off
@@ -437,10 +452,64 @@ def validate(args):
     print(json.dumps(out), flush=True)
 
 
+def c2p_batch(args):
+    """Learned con2prim on sampled states (rho log-uniform [1e-4, 10], p
+    [1e-6, 10], W [1, 50], isotropic v and B, sigma log-uniform [1e-3, 10],
+    Gamma 4/3): Newton steps after the guess, fallback rate, relative error of
+    the primitives against the full float64 Newton, and states/s of the
+    learned path, the same solver from the analytic start, and the
+    reference's con2prim."""
+    import torch
+    from astrofd_b200 import learned_c2p as LC
+    N = args.c2p_batch
+    e = LC.c2p_engine()
+    if args.c2p_jet:
+        from astrofd_b200.train_c2p_mlp import harvest_jet
+        prim = harvest_jet(n=128, steps=12, per_snapshot=-(-N // 4), seed=7)[:, :N].contiguous()
+        e = LC.c2p_engine(p_max=2.0)  # the jet's P_MAX
+    else:
+        prim = torch.as_tensor(LC.sample_primitives(N, 2024), device="cuda")
+    U = e.p2c_array(prim)
+    N = U.shape[1]
+    params = torch.as_tensor(LC.load(args.c2p_net or LC.DATA), dtype=torch.float32).cuda()
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return out, e0.elapsed_time(e1) / reps
+
+    ref, ms_ref = timed(lambda: e.c2p_array(U))
+    out = {"config": f"c2p batch, {N} " + ("states of a 128^3 jet run" if args.c2p_jet
+                                           else "sampled states"), "states": N}
+    for name, prm in (("learned", params), ("analytic_start", None)):
+        (q, st), ms = timed(lambda: LC.c2p_learned(e, U, prm, max_polish=2))
+        rel = ((q[:5] - ref[:5]).abs() / ref[:5].abs().clamp_min(1e-300)).amax(0)
+        n = st["cells"]
+        out[name] = {"states_per_s": N / (ms / 1e3), "ms": ms,
+                     "newton_steps_per_polished_state": st["polish_steps"] / max(n, 1),
+                     "polished_within_2": st["learned_polish"] / n,
+                     "fallback_rate": st["learned_fallback"] / n,
+                     "max_rel_err": float(rel.max()),
+                     "p999_rel_err": float(torch.quantile(rel[::max(1, N // 1000000)].float(), 0.999)),
+                     "frac_rel_err_gt_1e-6": float((rel > 1e-6).double().mean()),
+                     "status": st["status"]}
+    out["reference_c2p"] = {"states_per_s": N / (ms_ref / 1e3), "ms": ms_ref}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.validate_steps:
         validate(args)
+        return
+    if args.c2p_batch:
+        c2p_batch(args)
         return
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

@@ -226,9 +226,16 @@ int astro_mlp_adam(void* params, float* grad, float* m, float* v, float lr, floa
                    float beta2, float eps, int step, void* stream);
 /* con2prim of a (9, count) batch with the learned guess (p->mlp set); with
  * p->mlp == NULL the same polish/fallback runs from Z = D + tau + B^2 (the
- * reference's second Newton start), the no-network comparison */
+ * reference's second Newton start), the no-network comparison.  States whose
+ * polish fails get the reference's complete con2prim (cons_to_prim_rmhd,
+ * core/rmhd_core.py:249): with a workspace of
+ * astro_c2p_learned_workspace_bytes(count) bytes they are listed and solved
+ * by a second kernel; with work == NULL inline, where one slow state holds up
+ * its 128-state tile. */
+size_t astro_c2p_learned_workspace_bytes(int64_t count);
 int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
-                      int max_polish, AstroC2PStats* stats, int* status, void* stream);
+                      int max_polish, void* work, size_t work_bytes, AstroC2PStats* stats,
+                      int* status, void* stream);
 
 /* --- operator-split post-step sources (core/source_terms.py:5,30) -------- */
 int astro_cooling_heating(double* pr, const AstroGrid* g, int ng, double dt, double cool,
