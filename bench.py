@@ -362,9 +362,9 @@ def roofline(args, prof_ms, prof_n, prec, learned):
     N = n + 2 * ng
     rs = 4 if prec == "mixed" else 8
     if cls == 0:
-        # one direction: every face reads one new column of nm float64
-        # primitives and writes its nm fluxes
-        units, per_unit = (n + 1) * n * n, nm * 8 + nm * rs
+        # one direction: every face reads one new column of the nm primitives
+        # (the float32 copy in mixed precision) and writes its nm fluxes
+        units, per_unit = (n + 1) * n * n, nm * rs + nm * rs
     elif cls == 1:
         # every cell: 3 flux buffers, pr0 (nv), pr_k psi + passives, U_{k-1}
         # (stages 2-3), U_k, the next primitives (all nv, or the non-main ones
