@@ -374,7 +374,9 @@ def roofline(args, prof_ms, prof_n, prec, learned):
         dst = (nv - nm) * 8 if learned else nv * 8
         units, per_unit = N ** 3, 3 * nm * rs + nv * 8 + (npas + 1) * 8 + u_in + u_out + dst
     else:
-        units, per_unit = N ** 3, 2 * nm * 8  # U in, primitives out
+        # U in, primitives out, and in mixed precision the float32 copy of the
+        # primitives for the next stage's faces (written in 2 of 3 stages)
+        units, per_unit = N ** 3, 2 * nm * 8 + (2.0 / 3.0 * nm * rs if prec == "mixed" else 0)
     achieved = units * per_unit / avg_s / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
