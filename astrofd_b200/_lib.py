@@ -44,7 +44,7 @@ class AstroNozzle(C.Structure):
     _fields_ = [("ng", C.c_int32), ("profile", C.c_int32), ("perturb", C.c_int32),
                 ("physics", C.c_int32), ("b_init", C.c_int32), ("n_tracers", C.c_int32),
                 ("tracer_offset", C.c_int32), ("two_temperature", C.c_int32),
-                ("thermo_offset", C.c_int32), ("reserved", C.c_int32),
+                ("thermo_offset", C.c_int32), ("ambient_bc", C.c_int32),
                 ("radius", C.c_double), ("shear_thick", C.c_double),
                 ("gamma_jet", C.c_double), ("eta_rho", C.c_double), ("p_eq", C.c_double),
                 ("rho_amb", C.c_double), ("vx_amb", C.c_double), ("vy_amb", C.c_double),
@@ -52,7 +52,8 @@ class AstroNozzle(C.Structure):
                 ("turb_pamp", C.c_double), ("b0", C.c_double), ("te", C.c_double),
                 ("ti", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
                 ("y0", C.c_double), ("z0", C.c_double),
-                ("tracer_nozzle", C.c_double * 8), ("tracer_amb", C.c_double * 8)]
+                ("tracer_nozzle", C.c_double * 8), ("tracer_amb", C.c_double * 8),
+                ("b_amb_x", C.c_double)]
 
 
 class AstroC2PStats(C.Structure):
@@ -88,6 +89,7 @@ PROTOS = {
                                        _DP, _VP, C.c_size_t, _VP]),
     "astro_periodic_yz": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
     "astro_outflow_right_x": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
+    "astro_outflow_yz": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
     "astro_nozzle_left_x": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroNozzle),
                                       _DP, _VP, C.c_int32, _VP]),
     "astro_p2c": (C.c_int, [C.POINTER(AstroParams), _DP, _DP, C.c_int64, _VP]),

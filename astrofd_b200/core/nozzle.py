@@ -62,7 +62,9 @@ def nozzle_struct(cfg, dy, dz, y0, z0):
     c.perturb = 0 if cfg.get("NOZZLE_PERTURB", "none") == "none" else 1
     c.physics = 1 if cfg.get("PHYSICS") in ("rmhd", "grmhd") else 0
     b = cfg.get("B_INIT")
-    c.b_init = 1 if b == "poloidal" else (2 if b == "toroidal" else 0)
+    c.b_init = {"poloidal": 1, "toroidal": 2, "toroidal_phi": 3}.get(b, 0)
+    c.ambient_bc = 1 if cfg.get("NOZZLE_AMBIENT", "fixed") == "outflow" else 0
+    c.b_amb_x = float(cfg.get("B_AMB_X", 0.0))
     c.n_tracers = int(cfg.get("N_TRACERS", 0))
     if c.n_tracers > 8:
         raise _lib.AstroError("at most 8 tracers are supported")

@@ -1086,6 +1086,35 @@ __device__ double nozzle_weight(double r, double radius, double shear, int profi
     return r <= radius ? 1.0 : 0.0;
 }
 
+// zero-gradient y/z ghost fill: each ghost cell of the y/z frame of every x
+// plane gathers the nearest interior cell (race-free: sources are interior)
+__global__ void k_outflow_yz(double* pr, int nv, int nx, int ny, int nz, int ng) {
+    const int nyi = ny - 2 * ng;
+    const size_t frame = (size_t)ny * nz - (size_t)nyi * (nz - 2 * ng);
+    const size_t n = (size_t)nx * frame, nc = (size_t)nx * ny * nz;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t / frame);
+        const size_t q = t % frame;
+        int j, k;
+        const size_t rows = (size_t)2 * ng * nz;  // the 2 ng full y-ghost rows first
+        if (q < rows) {
+            const int r = (int)(q / nz);
+            j = r < ng ? r : ny - 2 * ng + r;
+            k = (int)(q % nz);
+        } else {  // then the z-ghost columns of the interior rows
+            const size_t u = q - rows;
+            j = ng + (int)(u / (2 * ng));
+            const int c = (int)(u % (2 * ng));
+            k = c < ng ? c : nz - 2 * ng + c;
+        }
+        const int js = j < ng ? ng : (j >= ny - ng ? ny - ng - 1 : j);
+        const int ks = k < ng ? ng : (k >= nz - ng ? nz - ng - 1 : k);
+        const size_t dst = ((size_t)i * ny + j) * nz + k, src = ((size_t)i * ny + js) * nz + ks;
+        for (int v = 0; v < nv; ++v) pr[(size_t)v * nc + dst] = pr[(size_t)v * nc + src];
+    }
+}
+
 __global__ void k_nozzle(double* pr, int nv, int nx, int ny, int nz, AstroNozzle c,
                          const double* draws, const int32_t* rank_map, int n_weighted) {
     const int ng = c.ng, nyl = ny - 2 * ng, nzl = nz - 2 * ng;
@@ -1097,6 +1126,12 @@ __global__ void k_nozzle(double* pr, int nv, int nx, int ny, int nz, AstroNozzle
         const double y = (j - ng + 0.5) * c.dy, z = (k - ng + 0.5) * c.dz;
         const double rr = sqrt((y - c.y0) * (y - c.y0) + (z - c.z0) * (z - c.z0));
         const double s = nozzle_weight(rr, c.radius, c.shear_thick, c.profile);
+        if (c.ambient_bc == 1 && !(s > 0.0)) {
+            // outside the nozzle: zero-gradient from the first interior layer
+            const size_t cell = ((size_t)g * ny + j) * nz + k, src = ((size_t)ng * ny + j) * nz + k;
+            for (int v = 0; v < nv; ++v) pr[(size_t)v * nc + cell] = pr[(size_t)v * nc + src];
+            continue;
+        }
         double rho = c.eta_rho * c.rho_amb * s + c.rho_amb * (1.0 - s);
         double p = c.p_eq;
         const double beta = sqrt(1.0 - 1.0 / (c.gamma_jet * c.gamma_jet));
@@ -1131,12 +1166,20 @@ __global__ void k_nozzle(double* pr, int nv, int nx, int ny, int nz, AstroNozzle
             pr[(size_t)(c.thermo_offset + 1) * nc + cell] = c.ti;
         }
         if (c.physics == 1) {
-            double Bx = 0.0, By = 0.0;
+            double Bx = 0.0, By = 0.0, Bz = 0.0;
             if (c.b_init == 1) Bx = c.b0 * s;
             else if (c.b_init == 2) By = c.b0 * s;
+            else if (c.b_init == 3) {
+                // toroidal B_phi(r) around the jet axis, on the ambient axial field
+                const double bphi = rr < c.radius ? c.b0 * rr / c.radius : c.b0 * c.radius / rr;
+                const double f = rr > 0.0 ? s * bphi / rr : 0.0;
+                Bx = c.b_amb_x;
+                By = -f * (z - c.z0);
+                Bz = f * (y - c.y0);
+            }
             pr[5 * nc + cell] = Bx;
             pr[6 * nc + cell] = By;
-            pr[7 * nc + cell] = 0.0;
+            pr[7 * nc + cell] = Bz;
             pr[8 * nc + cell] = 0.0;
         }
     }
@@ -1432,9 +1475,23 @@ int astro_nozzle_left_x(double* pr, const AstroGrid* g, const AstroNozzle* nz,
     if (nz->n_tracers > 0 && (nz->tracer_offset < 0 || nz->tracer_offset + nz->n_tracers > g->nv))
         return ASTRO_E_SHAPE;
     if (nz->two_temperature && nz->thermo_offset < 0) return ASTRO_E_SHAPE;
+    if (nz->b_init < 0 || nz->b_init > 3 || nz->ambient_bc < 0 || nz->ambient_bc > 1)
+        return ASTRO_E_INVALID;
+    if (nz->ambient_bc == 1 && g->nx <= nz->ng) return ASTRO_E_SHAPE;
     const size_t n = (size_t)nz->ng * (g->ny - 2 * nz->ng) * (g->nz - 2 * nz->ng);
     k_nozzle<<<grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(pr, g->nv, g->nx, g->ny, g->nz,
                                                                 *nz, draws, rank_map, n_weighted);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_outflow_yz(double* pr, const AstroGrid* g, int ng, void* stream) {
+    if (!pr || !g || ng < 1) return ASTRO_E_INVALID;
+    if (g->ny - 2 * ng < 1 || g->nz - 2 * ng < 1 || g->nx < 1) return ASTRO_E_SHAPE;
+    const size_t frame = (size_t)g->ny * g->nz - (size_t)(g->ny - 2 * ng) * (g->nz - 2 * ng);
+    const size_t n = (size_t)g->nx * frame;
+    k_outflow_yz<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(pr, g->nv, g->nx, g->ny,
+                                                                     g->nz, ng);
     mark(2, (cudaStream_t)stream);
     return cuda_status(cudaGetLastError());
 }

@@ -21,8 +21,17 @@ def _h(rho, p, gamma):
     return 1.0 + gamma / (gamma - 1.0) * p / rho
 
 
-def rmhd_jet_config(n, ng=3, vjet=0.995, sigma_amb=0.01, sigma_jet=0.5, radius=0.1):
-    """(core params, nozzle cfg, source cfg) of the magnetised jet."""
+def rmhd_jet_config(n, ng=3, vjet=0.995, sigma_amb=0.01, sigma_jet=0.5, radius=0.1,
+                    boundaries="reference"):
+    """(core params, nozzle cfg, source cfg) of the magnetised jet.
+
+    boundaries="reference": the reference driver's set-up (periodic y/z, fixed
+    ambient state on the x = 0 face outside the nozzle, the nozzle's
+    "toroidal" field By = B0 s with Bx = 0).  boundaries="baseline": the
+    magnetised configurations as specified (outflow on every face but the
+    nozzle, a toroidal B_phi = b0 r/R in the jet on the uniform ambient Bx),
+    with the library's extensions (astro_outflow_yz, nozzle b_init 3 and
+    ambient_bc 1); the nozzle cfg's YZ_BOUNDARY names the y/z fill."""
     W = 1.0 / math.sqrt(1.0 - vjet * vjet)
     rho_j, p_j = 0.1, 0.01
     # comoving b^2 = B^2 / W^2 for a field perpendicular to v
@@ -36,6 +45,11 @@ def rmhd_jet_config(n, ng=3, vjet=0.995, sigma_amb=0.01, sigma_jet=0.5, radius=0
                   PHYSICS="rmhd", B_INIT="toroidal", B0=b0, N_TRACERS=0,
                   TWO_TEMPERATURE=True, THERMO_OFFSET=9, TE_NOZZLE=p_j / rho_j,
                   TI_NOZZLE=p_j / rho_j)
+    if boundaries == "baseline":
+        nozzle.update(B_INIT="toroidal_phi", NOZZLE_AMBIENT="outflow", YZ_BOUNDARY="outflow",
+                      B_AMB_X=math.sqrt(sigma_amb * 1.0 * _h(1.0, 0.01, GAMMA_RMHD)))
+    elif boundaries != "reference":
+        raise ValueError(boundaries)
     sources = dict(COOLING_ENABLED=True, COOLING_LAMBDA=0.01, HEATING_RATE=0.0, NG=ng,
                    P_MAX=2.0, TWO_TEMPERATURE=True, TEI_TAU=0.1, THERMO_OFFSET=9,
                    N_TRACERS=0)

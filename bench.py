@@ -48,6 +48,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--flux-mode", default="conservative", choices=["conservative", "reference"])
+    ap.add_argument("--boundaries", default="baseline", choices=["baseline", "reference"],
+                    help="baseline: outflow on every face but the nozzle and a toroidal "
+                         "B_phi(r) jet field on the ambient Bx (the configuration as "
+                         "specified); reference: the reference driver's periodic y/z, "
+                         "fixed ambient inlet and By = B0 s")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -176,7 +181,10 @@ class DriverStep:
         self.rng = np.random.default_rng(1234)
 
     def bcs(self, pr):
-        self.B.apply_periodic_yz(pr, self.ng)
+        if self.noz.get("YZ_BOUNDARY") == "outflow":
+            self.B.apply_outflow_yz(pr, self.ng)
+        else:
+            self.B.apply_periodic_yz(pr, self.ng)
         self.B.apply_outflow_right_x(pr, self.ng)
         self.N.apply_nozzle_left_x(pr, self.d, self.d, self.d, self.n, self.n, 0.5, 0.5,
                                    self.rng, self.noz)
@@ -310,7 +318,7 @@ def cpu_sample(args, steps, warmup):
     import oracle as O
     from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
     n, ng, xc = args.n, 3, args.cpu_x_cells
-    core, noz, src = rmhd_jet_config(n, ng)
+    core, noz, src = rmhd_jet_config(n, ng, boundaries=args.boundaries)
     # the reference's own arithmetic (loop-carried x-face speeds, its resistive
     # handling), whatever flux mode the GPU arm runs
     cfg = dict(core, FLUX_MODE="reference")
@@ -321,7 +329,10 @@ def cpu_sample(args, steps, warmup):
     rng = np.random.default_rng(1234)
 
     def bcs(a):
-        O.apply_periodic_yz(a, ng)
+        if noz.get("YZ_BOUNDARY") == "outflow":
+            O.apply_outflow_yz(a, ng)
+        else:
+            O.apply_periodic_yz(a, ng)
         O.apply_outflow_right_x(a, ng)
         O.apply_nozzle_left_x(a, d, d, d, n, n, 0.5, 0.5, rng, noz)
 
@@ -401,7 +412,7 @@ def validate(args):
     from astrofd_b200.core import rmhd_core
     from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
     n, K = args.n, args.validate_steps
-    cfgs = rmhd_jet_config(n, 3)
+    cfgs = rmhd_jet_config(n, 3, boundaries=args.boundaries)
     core, noz, src = cfgs
 
     def run(prec, learned, perturb=0.0):
@@ -528,7 +539,8 @@ def main():
                 "impl": "reference", "dtype": "f64", "data": "synthetic",
                 "config": {"workload": f"rmhd-jet-{args.n}^3 weno5/hlld ssprk3 + resistive + "
                                        "two-temperature + cooling", "sample_x_cells":
-                               args.cpu_x_cells, "flux_mode": "reference"},
+                               args.cpu_x_cells, "flux_mode": "reference",
+                               "boundaries": args.boundaries},
                 "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"],
                                  "kind": r["kind"], "sample": r["sample"]},
                 "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -541,7 +553,7 @@ def main():
     from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
     rank, world, local = dist_init(args)
     n = args.n
-    cfgs = rmhd_jet_config(n, 3)
+    cfgs = rmhd_jet_config(n, 3, boundaries=args.boundaries)
     pr_host = rmhd_jet(n, 3, seed=2024 + rank)
     zones = n ** 3 * args.steps * world
 
@@ -568,7 +580,7 @@ def main():
                                "two-temperature + cooling (driver-loop iteration)",
                    "grid": [n, n, n], "ng": 3, "nv": 11, "precision": "mixed",
                    "c2p_guess": "learned" if learned else "reference",
-                   "flux_mode": args.flux_mode,
+                   "flux_mode": args.flux_mode, "boundaries": args.boundaries,
                    "l2": "inputs larger than L2 (1.6 GB arrays)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "gpu_launches": mixed["launches"],

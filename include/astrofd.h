@@ -88,12 +88,19 @@ typedef struct AstroGrid {
 typedef struct AstroNozzle {
     int32_t ng, profile;        /* profile 0 top_hat, 1 taper, 2 parabolic          */
     int32_t perturb, physics;   /* perturb != 0: draws supplied; physics 1 = rmhd   */
-    int32_t b_init;             /* 0 none, 1 poloidal (Bx), 2 toroidal (By = B0 s)  */
-    int32_t n_tracers, tracer_offset, two_temperature, thermo_offset, reserved;
+    int32_t b_init;             /* 0 none, 1 poloidal (Bx), 2 toroidal (By = B0 s),
+                                   3 B_phi(r) = B0 r/R (r < R), B0 R/r (r >= R),
+                                     times s, plus Bx = b_amb_x (no reference
+                                     counterpart)                                 */
+    int32_t n_tracers, tracer_offset, two_temperature, thermo_offset;
+    int32_t ambient_bc;         /* cells with s = 0: 0 the fixed ambient state (the
+                                   reference), 1 zero-gradient copy of the first
+                                   interior x layer (no reference counterpart)    */
     double radius, shear_thick, gamma_jet, eta_rho, p_eq, rho_amb;
     double vx_amb, vy_amb, vz_amb, turb_vamp, turb_pamp, b0, te, ti;
     double dy, dz, y0, z0;
     double tracer_nozzle[8], tracer_amb[8];
+    double b_amb_x;             /* axial ambient field carried through the inlet (b_init 3) */
 } AstroNozzle;
 
 /* con2prim outcome counters accumulated by astro_step/astro_c2p */
@@ -190,6 +197,14 @@ int astro_outflow_right_x(double* pr, const AstroGrid* g, int ng, void* stream);
 int astro_nozzle_left_x(double* pr, const AstroGrid* g, const AstroNozzle* nz,
                         const double* draws, const int32_t* rank_map, int32_t n_weighted,
                         void* stream);
+
+/* Zero-gradient ("outflow") ghost fill of the four y and z faces over the
+ * whole x extent: every ghost cell takes the value of the nearest interior
+ * cell in y and z (the same as copying the y layers first, then the z layers).
+ * No counterpart in the reference, whose driver fills y and z periodically
+ * (astro_periodic_yz); jet set-ups with outflow on every face but the nozzle
+ * use this instead. */
+int astro_outflow_yz(double* pr, const AstroGrid* g, int ng, void* stream);
 
 /* --- pointwise conversions ----------------------------------------------
  * Array forms of prim_to_cons / cons_to_prim (core/srhd_core.py:47,62) and

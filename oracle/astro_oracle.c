@@ -1096,6 +1096,26 @@ void oracle_periodic_yz(double* pr, int nv, int nx, int ny, int nz, int ng) {
             }
 }
 
+/* extension, no reference counterpart: zero-gradient y faces, then z faces */
+void oracle_outflow_yz(double* pr, int nv, int nx, int ny, int nz, int ng) {
+    OGrid g0 = {nv, nx, ny, nz};
+    const OGrid* g = &g0;
+    for (int v = 0; v < nv; ++v)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ng; ++j)
+                for (int k = 0; k < nz; ++k) {
+                    P(v, i, j, k) = P(v, i, ng, k);
+                    P(v, i, ny - 1 - j, k) = P(v, i, ny - 1 - ng, k);
+                }
+    for (int v = 0; v < nv; ++v)
+        for (int i = 0; i < nx; ++i)
+            for (int j = 0; j < ny; ++j)
+                for (int k = 0; k < ng; ++k) {
+                    P(v, i, j, k) = P(v, i, j, ng);
+                    P(v, i, j, nz - 1 - k) = P(v, i, j, nz - 1 - ng);
+                }
+}
+
 void oracle_outflow_right_x(double* pr, int nv, int nx, int ny, int nz, int ng) {
     OGrid g0 = {nv, nx, ny, nz};
     const OGrid* g = &g0;
@@ -1109,12 +1129,13 @@ typedef struct {
     int ng, profile;          /* profile 0 top_hat, 1 taper/smooth, 2 parabolic */
     int perturb;              /* 0 none, else random                            */
     int physics;              /* 0 hydro, 1 rmhd                                */
-    int b_init;               /* 0 none, 1 poloidal, 2 toroidal                 */
+    int b_init;               /* 0 none, 1 poloidal, 2 toroidal, 3 B_phi(r)     */
     int n_tracers, tracer_offset, two_temperature, thermo_offset;
-    int pad_;
+    int ambient_bc;           /* s = 0 cells: 0 fixed ambient, 1 zero-gradient  */
     double radius, shear_thick, gamma_jet, eta_rho, p_eq, rho_amb;
     double vx_amb, vy_amb, vz_amb, turb_vamp, turb_pamp, b0, te, ti;
     double tracer_nozzle[8], tracer_amb[8];
+    double b_amb_x;
 } ONozzle;
 
 static double nozzle_weight(double r, double radius, double shear, int profile) {
@@ -1147,6 +1168,11 @@ long oracle_nozzle_left_x(double* pr, int nv, int nx, int ny, int nz, double dy,
                 double z = (k - c->ng + 0.5) * dz;
                 double rr = sqrt((y - y0) * (y - y0) + (z - z0) * (z - z0));
                 double s = nozzle_weight(rr, c->radius, c->shear_thick, c->profile);
+                /* extension, no reference counterpart: outflow outside the nozzle */
+                if (c->ambient_bc == 1 && !(s > 0.0)) {
+                    for (int v = 0; v < nv; ++v) P(v, gg, j, k) = P(v, c->ng, j, k);
+                    continue;
+                }
                 double rho = c->eta_rho * c->rho_amb * s + c->rho_amb * (1.0 - s);
                 double p = c->p_eq;
                 double beta = sqrt(1.0 - 1.0 / (c->gamma_jet * c->gamma_jet));
@@ -1171,10 +1197,19 @@ long oracle_nozzle_left_x(double* pr, int nv, int nx, int ny, int nz, double dy,
                     P(c->thermo_offset + 1, gg, j, k) = c->ti;
                 }
                 if (c->physics == 1) {
-                    double Bx = 0.0, By = 0.0;
+                    double Bx = 0.0, By = 0.0, Bz = 0.0;
                     if (c->b_init == 1) Bx = c->b0 * s;
                     else if (c->b_init == 2) By = c->b0 * s;
-                    P(5, gg, j, k) = Bx; P(6, gg, j, k) = By; P(7, gg, j, k) = 0.0;
+                    else if (c->b_init == 3) {
+                        /* extension: B_phi = B0 r/R inside, B0 R/r outside, times s */
+                        double bphi = rr < c->radius ? c->b0 * rr / c->radius
+                                                     : c->b0 * c->radius / rr;
+                        double f = rr > 0.0 ? s * bphi / rr : 0.0;
+                        Bx = c->b_amb_x;
+                        By = -f * (z - z0);
+                        Bz = f * (y - y0);
+                    }
+                    P(5, gg, j, k) = Bx; P(6, gg, j, k) = By; P(7, gg, j, k) = Bz;
                     P(8, gg, j, k) = 0.0;
                 }
             }

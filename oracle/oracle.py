@@ -32,7 +32,7 @@ class ONozzle(C.Structure):
     _fields_ = [("ng", C.c_int), ("profile", C.c_int), ("perturb", C.c_int),
                 ("physics", C.c_int), ("b_init", C.c_int), ("n_tracers", C.c_int),
                 ("tracer_offset", C.c_int), ("two_temperature", C.c_int),
-                ("thermo_offset", C.c_int), ("pad_", C.c_int),
+                ("thermo_offset", C.c_int), ("ambient_bc", C.c_int),
                 ("radius", C.c_double), ("shear_thick", C.c_double),
                 ("gamma_jet", C.c_double), ("eta_rho", C.c_double),
                 ("p_eq", C.c_double), ("rho_amb", C.c_double),
@@ -40,7 +40,7 @@ class ONozzle(C.Structure):
                 ("vz_amb", C.c_double), ("turb_vamp", C.c_double),
                 ("turb_pamp", C.c_double), ("b0", C.c_double), ("te", C.c_double),
                 ("ti", C.c_double), ("tracer_nozzle", C.c_double * 8),
-                ("tracer_amb", C.c_double * 8)]
+                ("tracer_amb", C.c_double * 8), ("b_amb_x", C.c_double)]
 
 
 _lib = None
@@ -67,7 +67,7 @@ def lib():
         L.oracle_c2p_counters.argtypes = [C.POINTER(C.c_long), C.c_int]
         L.oracle_max_char_speed.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int]
         L.oracle_max_char_speed.restype = C.c_double
-        for f in (L.oracle_periodic_yz, L.oracle_outflow_right_x):
+        for f in (L.oracle_periodic_yz, L.oracle_outflow_right_x, L.oracle_outflow_yz):
             f.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.oracle_nozzle_left_x.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int,
                                            C.c_double, C.c_double, C.c_int, C.c_int,
@@ -164,6 +164,12 @@ def apply_periodic_yz(pr, ng):
     lib().oracle_periodic_yz(_dp(pr), *pr.shape, ng)
 
 
+def apply_outflow_yz(pr, ng):
+    """Zero-gradient y and z faces (an extension; the reference has none)."""
+    assert pr.flags.c_contiguous and pr.dtype == np.float64
+    lib().oracle_outflow_yz(_dp(pr), *pr.shape, ng)
+
+
 def apply_outflow_right_x(pr, ng):
     assert pr.flags.c_contiguous and pr.dtype == np.float64
     lib().oracle_outflow_right_x(_dp(pr), *pr.shape, ng)
@@ -179,7 +185,9 @@ def nozzle_struct(cfg):
     c.perturb = 0 if cfg.get("NOZZLE_PERTURB", "none") == "none" else 1
     c.physics = 1 if cfg.get("PHYSICS") in ("rmhd", "grmhd") else 0
     b = cfg.get("B_INIT")
-    c.b_init = 1 if b == "poloidal" else (2 if b == "toroidal" else 0)
+    c.b_init = {"poloidal": 1, "toroidal": 2, "toroidal_phi": 3}.get(b, 0)
+    c.ambient_bc = 1 if cfg.get("NOZZLE_AMBIENT", "fixed") == "outflow" else 0
+    c.b_amb_x = float(cfg.get("B_AMB_X", 0.0))
     c.n_tracers = int(cfg.get("N_TRACERS", 0))
     c.tracer_offset = int(cfg.get("TRACER_OFFSET", 5))
     c.two_temperature = 1 if cfg.get("TWO_TEMPERATURE", False) else 0
