@@ -8,7 +8,8 @@ magnetised-jet parameters of the RMHD configurations).
                          rho=1, p=0.01, uniform Bx with sigma=0.01, 1 % seeded
                          velocity noise; the jet (rho=0.1, vx=0.995, W=10.01)
                          enters through the left-x nozzle with a toroidal field.
-    srhd_jet(n, ng)      SRHD, ambient rho=1(1 + 1 % noise), p=0.01, at rest.
+    srhd_jet(n, ng)      SRHD, ambient rho=1(1 + 1 % noise), p=0.01, at rest;
+                         srhd_jet_config gives its nozzle and scheme.
 """
 import math
 
@@ -71,6 +72,29 @@ def rmhd_jet(n, ng=3, seed=2024, sigma_amb=0.01, x_cells=None):
     pr[9] = 0.01
     pr[10] = 0.01
     return pr
+
+
+def srhd_jet_config(n, ng=2, vjet=0.99, recon="muscl", limiter="minmod", riemann="hlle",
+                    rk_order=2, cfl=0.4, radius=0.1, boundaries="reference"):
+    """(core params, nozzle cfg) of the SRHD jet: Gamma = 5/3, ambient rho = 1
+    (1 % noise), p = 0.01 at rest, nozzle rho = 0.1, p = 0.01, vx = vjet on the
+    x = 0 face.  The defaults are the 64^3 MUSCL-minmod/HLLE/SSPRK2 set-up;
+    vjet=0.995, recon="ppm", riemann="hllc", rk_order=3 the 128^3 one.
+    boundaries as in rmhd_jet_config ("baseline": outflow on every face but the
+    nozzle)."""
+    W = 1.0 / math.sqrt(1.0 - vjet * vjet)
+    core = dict(GAMMA=5.0 / 3.0, P_MAX=2.0, V_MAX=0.9999, RECON=recon, LIMITER=limiter,
+                RIEMANN=riemann, RK_ORDER=rk_order, CFL=cfl, N_PASSIVE=0, PASSIVE_OFFSET=5)
+    nozzle = dict(NG=ng, JET_RADIUS=radius, SHEAR_THICK=0.0, NOZZLE_PROFILE="top_hat",
+                  GAMMA_JET=W, ETA_RHO=0.1, P_EQ=0.01, RHO_AMB=1.0, VX_AMB=0.0, VY_AMB=0.0,
+                  VZ_AMB=0.0, NOZZLE_PERTURB="none", TURB_VAMP=0.0, TURB_PAMP=0.0,
+                  PHYSICS="hydro", B_INIT="none", B0=0.0, N_TRACERS=0,
+                  TWO_TEMPERATURE=False)
+    if boundaries == "baseline":
+        nozzle.update(NOZZLE_AMBIENT="outflow", YZ_BOUNDARY="outflow")
+    elif boundaries != "reference":
+        raise ValueError(boundaries)
+    return core, nozzle
 
 
 def srhd_jet(n, ng=2, seed=2024):

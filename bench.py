@@ -62,6 +62,8 @@ def parse():
                     help="learned con2prim weights (.npz); default: the packaged network")
     ap.add_argument("--no-learned", action="store_true",
                     help="headline arm without the learned con2prim guess")
+    ap.add_argument("--validate-srhd", action="store_true",
+                    help="with --validate-steps: the SRHD jet (PPM + HLLC, SSPRK3, v 0.995)")
     ap.add_argument("--c2p-batch", type=int, default=0, metavar="STATES",
                     help="learned con2prim on a batch of sampled states (2^24 for the "
                          "batch config) against the full float64 Newton, then exit")
@@ -405,6 +407,65 @@ def roofline(args, prof_ms, prof_n, prec, learned):
             "class_share": round(float(prof_ms[cls] / max(prof_ms.sum(), 1e-30)), 3)}
 
 
+def _norms(a, b, ng):
+    """Relative L1 and Linf of rho, p and W of state a against state b over
+    the interior."""
+    import torch
+    i = slice(ng, -ng)
+
+    def fields(q):
+        q = q[:, i, i, i]
+        return {"rho": q[0], "p": q[4],
+                "W": 1.0 / torch.sqrt(1.0 - (q[1] ** 2 + q[2] ** 2 + q[3] ** 2))}
+
+    fa, fb = fields(a), fields(b)
+    return {k: {"l1": float(((fa[k] - fb[k]).abs().mean() / fb[k].abs().mean()).item()),
+                "linf": float(((fa[k] - fb[k]).abs().max() / fb[k].abs().max()).item())}
+            for k in fb}
+
+
+def validate_srhd(args):
+    """Accuracy of the mixed-precision SRHD jet (PPM + HLLC, SSPRK3, v_jet
+    0.995, CFL 0.4 with the reference's amax rule) against plain float64, with
+    the float64 perturbation floor beside it."""
+    import torch
+    from astrofd_b200.core import boundary, nozzle, srhd_core
+    from astrofd_b200.workloads import srhd_jet, srhd_jet_config
+    n, K, ng = args.n, args.validate_steps, 3
+    core, noz = srhd_jet_config(n, ng, vjet=0.995, recon="ppm", riemann="hllc", rk_order=3,
+                                boundaries=args.boundaries)
+    d = 1.0 / n
+    yz = boundary.apply_outflow_yz if noz.get("YZ_BOUNDARY") == "outflow" else \
+        boundary.apply_periodic_yz
+
+    def run(prec, perturb=0.0):
+        srhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode))
+        pr = srhd_jet(n, ng)
+        if perturb:
+            pr[0] *= 1.0 + perturb * np.random.default_rng(5).standard_normal(pr[0].shape)
+        a = torch.from_numpy(pr).cuda()
+        rng = np.random.default_rng(1234)
+        N = a.shape[1]
+
+        def bcs(t):
+            yz(t, ng)
+            boundary.apply_outflow_right_x(t, ng)
+            nozzle.apply_nozzle_left_x(t, d, d, d, n, n, 0.5, 0.5, rng, noz)
+        for _ in range(K):
+            dt = core["CFL"] * d / max(srhd_core.max_char_speed(a, N, N, N), 1e-12)
+            bcs(a)
+            a = srhd_core.step_ssprk3(a, d, d, d, dt)
+            bcs(a)
+        return a
+
+    ref = run("fp64")
+    out = {"validate_steps": K, "grid": n, "physics": "srhd ppm/hllc ssprk3",
+           "flux_mode": args.flux_mode, "boundaries": args.boundaries,
+           "mixed_vs_fp64": _norms(run("mixed"), ref, ng),
+           "fp64_perturbed_1e-12_vs_fp64": _norms(run("fp64", 1e-12), ref, ng)}
+    print(json.dumps(out), flush=True)
+
+
 def validate(args):
     """Accuracy protocol of the mixed + learned path against plain float64."""
     import torch
@@ -434,21 +495,10 @@ def validate(args):
     ref, st_ref = run("fp64", False)
     mix, st_mix = run("mixed", True)
     per, _ = run("fp64", False, perturb=1e-12)
-    i = slice(3, -3)
 
-    def fields(q):
-        q = q[:, i, i, i]
-        return {"rho": q[0], "p": q[4],
-                "W": 1.0 / torch.sqrt(1.0 - (q[1] ** 2 + q[2] ** 2 + q[3] ** 2))}
-
-    def norms(a, b):
-        fa, fb = fields(a), fields(b)
-        return {k: {"l1": float(((fa[k] - fb[k]).abs().mean() / fb[k].abs().mean()).item()),
-                    "linf": float(((fa[k] - fb[k]).abs().max() / fb[k].abs().max()).item())}
-                for k in fb}
-
-    nm, npr = norms(mix, ref), norms(per, ref)
+    nm, npr = _norms(mix, ref, 3), _norms(per, ref, 3)
     out = {"validate_steps": K, "grid": n, "flux_mode": args.flux_mode,
+           "boundaries": args.boundaries,
            "rho_l1_mixed_learned_vs_fp64": nm["rho"]["l1"],
            "rho_l1_fp64_perturbed_1e-12_vs_fp64": npr["rho"]["l1"],
            "mixed_learned_vs_fp64": nm, "fp64_perturbed_1e-12_vs_fp64": npr,
@@ -524,7 +574,7 @@ def c2p_batch(args):
 def main():
     args = parse()
     if args.validate_steps:
-        validate(args)
+        (validate_srhd if args.validate_srhd else validate)(args)
         return
     if args.c2p_batch:
         c2p_batch(args)
