@@ -618,10 +618,11 @@ __device__ __forceinline__ void c2p_features(const double* U, float* x) {
     const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
     const double iD = 1.0 / D;
     const double r[4] = {sqrt(S2) * iD, rmax(U[4], 0.0) * iD, B2 * iD, SB * SB * iD * iD * iD};
-    // the features feed a float32/bfloat16 network: float32 logarithms
-    x[0] = logf((float)rmax(D, 1e-30));
+    // the features feed a bfloat16 network (8-bit mantissa): the fast
+    // float32 logarithm (one MUFU operation) is far more accurate than that
+    x[0] = __logf((float)rmax(D, 1e-30));
 #pragma unroll
-    for (int i = 0; i < 4; ++i) x[1 + i] = log1pf((float)rmin(r[i], 1e30));
+    for (int i = 0; i < 4; ++i) x[1 + i] = __logf(1.0f + (float)rmin(r[i], 1e30));
 }
 
 struct C2PArgs {
