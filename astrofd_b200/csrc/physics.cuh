@@ -781,23 +781,67 @@ AHD void r_c2p_start(const Phys<double>& P, const double* U, double* q0, double&
     Z1 = rmax(D + tau + B2, SM);
 }
 
-// At most max_steps Newton steps of the reference's update rule (forward-
-// difference derivative, +-Z/2 clamp), testing |f| < 1e-10 max(1, tau) before
-// each step and after the last.  *steps = steps taken when converged.
+// f(Z) of the reference's con2prim equation (the same arithmetic as
+// r_f_of_Z) and, when df is non-null, its analytic derivative from the same
+// intermediates: v^2 = A / Bq with A = S^2 + (S.B)^2 (2Z + B^2) / Z^2 and
+// Bq = (Z + B^2)^2, W^2 = 1 / (1 - v^2), rho = D / W, p = (G-1)/G (Z / W^2 - rho),
+// b^2 = B^2 / W^2 + (S.B / Z)^2.  Where the reference clamps v^2 or p the
+// clamped quantity is constant and contributes nothing.
+AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
+                       double SB, double S2, double* df) {
+    const double G = P.gamma, SM = 1e-12;
+    const double denomZ = rmax(Z, SM);
+    const double vb = SB / denomZ;
+    const double ZpB = Z + B2;
+    const double Bq = ZpB * ZpB + SM;
+    double v2 = (S2 + (SB * SB) * (2.0 * Z + B2) / (denomZ * denomZ)) / Bq;
+    const double vmax2 = P.v_max * P.v_max;
+    const bool vcap = v2 >= vmax2;
+    if (vcap) v2 = vmax2 - 1e-14;
+    const double W2 = 1.0 / (1.0 - v2);
+    const double W = sqrt(W2);
+    const double rho = D / rmax(W, SM);
+    const double h = Z / rmax(rho * W2, SM);
+    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    bool pcap = false;
+    if (p < SM) { p = SM; pcap = true; }
+    if (p > P.p_max) { p = P.p_max; pcap = true; }
+    const double b2 = B2 / W2 + vb * vb;
+    const double f = (Z - p + 0.5 * B2 + 0.5 * b2 - D) - tau;
+    if (df) {
+        const bool zfloor = Z < SM;
+        const double iZ = 1.0 / denomZ;
+        const double dA = zfloor ? 0.0 : -2.0 * SB * SB * ZpB * iZ * iZ * iZ;
+        const double dv2 = vcap ? 0.0 : (dA - v2 * 2.0 * ZpB) / Bq;
+        const double dW2 = W2 * W2 * dv2;
+        const double drho = -0.5 * rho * dW2 / W2;  // rho = D W2^-1/2
+        const double dp = pcap ? 0.0 : (G - 1.0) / G * (1.0 / W2 - Z * dW2 / (W2 * W2) - drho);
+        const double dvb = zfloor ? 0.0 : -vb * iZ;
+        const double db2 = -B2 * dW2 / (W2 * W2) + 2.0 * vb * dvb;
+        *df = 1.0 - dp + 0.5 * db2;
+    }
+    return f;
+}
+
+// At most max_steps Newton steps on the reference's con2prim equation with its
+// +-Z/2 step clamp and Z floor, the derivative analytic (r_f_df_of_Z: one
+// evaluation per step instead of the reference's two for a forward
+// difference), testing |f| < 1e-10 max(1, tau) before each step and after
+// the last.  *steps = steps taken when converged.  The converged Z meets the
+// reference's own criterion, so the result agrees with the reference's to
+// its tolerance.
 AHD bool r_newton_polish(const Phys<double>& P, double& Z, int max_steps, double D, double tau,
                          double B2, double SB, double S2, int* steps) {
     const double tol = 1e-10 * rmax(1.0, tau);
     for (int s = 0;; ++s) {
-        double f = r_f_of_Z(P, Z, D, tau, B2, SB, S2);
+        double dfdZ = 0.0;
+        const double f = r_f_df_of_Z(P, Z, D, tau, B2, SB, S2, s < max_steps ? &dfdZ : nullptr);
         if (fabs(f) < tol) {
             *steps = s;
             return true;
         }
         if (s == max_steps) break;
-        double eps = 1e-6 * rmax(1.0, Z);
-        double fp = r_f_of_Z(P, Z + eps, D, tau, B2, SB, S2);
-        double dfdZ = (fp - f) / eps;
-        if (dfdZ == 0.0) break;
+        if (dfdZ == 0.0 || !isfinite(dfdZ)) break;
         double dZ = -f / dfdZ;
         if (dZ > 0.5 * Z) dZ = 0.5 * Z;
         if (dZ < -0.5 * Z) dZ = -0.5 * Z;

@@ -83,26 +83,39 @@ def test_learned_c2p_matches_reference_and_beats_no_network():
     tr.train(X, T, steps=3000, batch=8192, lr=3e-3, lr_end=2e-4)
 
     # states with v.B = 0: the residual has one physical root, so the learned
-    # path (any start, same Newton update and tolerance) lands on the
-    # reference's solution
+    # path (any start, Newton to the reference's tolerance) lands on the
+    # reference's solution, to that tolerance: |f| < 1e-10 max(1, tau) pins Z
+    # to ~3e-10 max(1, tau) (f' >~ 0.75), hence rho and v to ~1e-9 relative
+    # (times W^2 <= 2500 for rho) and p to ~3e-10 max(1, tau) absolute -- not
+    # relative: p << tau on much of the sampler
     _, _, Up = LC.make_dataset(_perpendicular(LC.sample_primitives(20000, 8)), e)
     ref = e.c2p_array(Up).cpu().numpy()
     q, st = LC.c2p_learned(e, Up, tr.params, max_polish=2)
-    rel = np.abs(q.cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-300)
     assert st["status"] == 0 and st["cells"] == Up.shape[1]
-    assert np.all(rel[5:] == 0.0)
-    # both solutions meet |f| < 1e-10 max(1, tau), which leaves p free to
-    # ~1e-5 relative when tau >> p; beyond 1e-4 would mean another root
-    assert (rel[:5].max(axis=0) > 1e-4).mean() < 1e-2
+    q = q.cpu().numpy()
+    assert np.all(q[5:] == ref[5:])
+    off = _off_tolerance(q, ref, Up[4].cpu().numpy())
+    assert off.mean() < 1e-3, off.mean()
 
     # random v.B: the reference's p2c and c2p disagree there (its residual uses
     # b^2 = B^2/W^2 + (S.B/Z)^2), f(Z) can have several roots and the one found
     # depends on the start; the bulk still agrees to the Newton tolerance
     ref = e.c2p_array(U).cpu().numpy()
     q, st = LC.c2p_learned(e, U, tr.params, max_polish=2)
-    rel = np.abs(q.cpu().numpy() - ref) / np.maximum(np.abs(ref), 1e-300)
     assert st["status"] == 0 and st["cells"] == U.shape[1]
-    assert (rel[:5].max(axis=0) > 1e-4).mean() < 0.05
+    off = _off_tolerance(q.cpu().numpy(), ref, U[4].cpu().numpy())
+    assert off.mean() < 0.05, off.mean()
+
+
+def _off_tolerance(q, ref, tau):
+    """States whose primitives differ from the reference's by more than the
+    con2prim tolerance allows: rho or |v| beyond 1e-5 relative, p beyond
+    1e-8 max(1, tau) absolute."""
+    d_rho = np.abs(q[0] - ref[0]) / np.abs(ref[0])
+    d_v = np.linalg.norm(q[1:4] - ref[1:4], axis=0) / np.maximum(
+        np.linalg.norm(ref[1:4], axis=0), 1e-300)
+    d_p = np.abs(q[4] - ref[4]) / np.maximum(1.0, tau)
+    return (np.maximum(d_rho, d_v) > 1e-5) | (d_p > 1e-8)
 
 
 
