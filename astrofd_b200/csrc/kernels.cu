@@ -338,56 +338,23 @@ template <typename RF> __device__ __forceinline__ double ldf(const void* p, size
     return (double)__ldg((const RF*)p + i);
 }
 
-// asynchronous global -> shared copies of one 4- or 8-byte value (cp.async);
-// the issuing thread reads its own copies after cp_async_wait_all
-template <typename T> __device__ __forceinline__ void cp_async(T* s, const T* g) {
-    static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte values");
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
-    if constexpr (sizeof(T) == 4)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-// wait until at most one committed group of this thread is in flight
-__device__ __forceinline__ void cp_async_wait_but_one() {
-    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-}
-
-// Staged update (DEFER): shared memory per thread holds the 6*NM face fluxes
-// of its cell, then the float64 values it reads once: q0[NM], U_k[NM], psi
-// and the three B components of the stage input, passives t0[np], t_k[np].
 constexpr int kUpdateBlock = 128;
-inline size_t update_smem_bytes(int nm, size_t rf_bytes, int np) {
-    return ((size_t)6 * nm * rf_bytes + (size_t)(2 * nm + 4 + 2 * np) * 8) * kUpdateBlock;
-}
 
 // DEFER: the learned con2prim runs in its own kernel, so this one only writes
-// U (the con2prim code is compiled out, which frees registers), and every
-// value a cell reads once is first copied to shared memory with cp.async, all
-// of a thread's copies in flight together, so that the pass is bound by HBM
-// bandwidth rather than by the latency of one dependent load after another.
+// U (the con2prim code is compiled out, which frees registers for loads in
+// flight: 6 blocks of 128 threads per SM).  Every load is a plain coalesced
+// load with no dependence on an earlier one, so a thread's loads overlap each
+// other; staging them through shared memory with per-thread cp.async streamed
+// more slowly on B200 (4.2 against 6.4 TB/s for the same bytes).
 template <int PHYS, typename RF, bool DEFER, bool PASSIVE>
-__global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k_update(UpdArgs a) {
+__global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
     constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
-    constexpr bool STAGE = DEFER;
     constexpr int T = kUpdateBlock;
-    extern __shared__ __align__(16) unsigned char ush[];
     const unsigned nc32 = (unsigned)a.nx * (unsigned)a.ny * (unsigned)a.nz;
     const size_t nc = nc32;
     const unsigned cell32 = blockIdx.x * T + threadIdx.x;
     const size_t cell = cell32;
-    const int tid = threadIdx.x;
-    RF* sF = reinterpret_cast<RF*>(ush);
-    double* sD = reinterpret_cast<double*>(ush + (size_t)6 * NM * sizeof(RF) * T);
     const int np = a.p.n_passive, po = a.p.passive_offset;
-    // float64 item slots
-    const int I_U = NM, I_PSI = 2 * NM, I_B = 2 * NM + 1, I_T0 = 2 * NM + 4, I_TK = 2 * NM + 4 + np;
     C2PCount cnt;
     if (cell32 < nc32) {
         const unsigned k = cell32 % (unsigned)a.nz;
@@ -406,44 +373,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                        ? 1
                        : (a.p.recon == ASTRO_RECON_MUSCL ? 1 : (a.p.recon == ASTRO_RECON_PPM ? 2 : 0));
         }
-        if constexpr (STAGE) {
-            if (in) {
-#pragma unroll
-                for (int d = 0; d < 3; ++d)
-#pragma unroll
-                    for (int v = 0; v < NM; ++v) {
-                        const size_t o = (size_t)v * nc + cell;
-                        const RF* lo = (const RF*)(d == 0 ? a.FxL : a.F[d]);
-                        cp_async(&sF[((d * NM + v) * 2 + 1) * T + tid], (const RF*)a.F[d] + o + st[d]);
-                        cp_async(&sF[((d * NM + v) * 2 + 0) * T + tid], lo + o);
-                    }
-                if (PHYS == ASTRO_RMHD) {
-                    cp_async(&sD[I_PSI * T + tid], a.prk + 8 * nc + cell);
-                    if (nres)
-#pragma unroll
-                        for (int c = 0; c < 3; ++c)
-                            cp_async(&sD[(I_B + c) * T + tid], a.prk + (size_t)(5 + c) * nc + cell);
-                }
-            }
-            // two groups: the divergence runs while the RK operands arrive
-            cp_async_commit();
-            if (!a.rhs_only) {
-#pragma unroll
-                for (int v = 0; v < NM; ++v) {
-                    cp_async(&sD[v * T + tid], a.pr0 + (size_t)v * nc + cell);
-                    if (a.stage) cp_async(&sD[(I_U + v) * T + tid], a.U + (size_t)v * nc + cell);
-                }
-                for (int t = 0; t < np; ++t) {
-                    const size_t o = (size_t)(po + t) * nc + cell;
-                    cp_async(&sD[(I_T0 + t) * T + tid], a.pr0 + o);
-                    if (a.stage) cp_async(&sD[(I_TK + t) * T + tid], a.prk + o);
-                }
-            }
-            cp_async_commit();
-            cp_async_wait_but_one();
-        }
         auto flux = [&](int d, int v, int hi) -> double {
-            if constexpr (STAGE) return (double)sF[((d * NM + v) * 2 + hi) * T + tid];
             const size_t o = (size_t)v * nc + cell;
             if (hi) return ldf<RF>(a.F[d], o + st[d]);
             return ldf<RF>(d == 0 ? a.FxL : a.F[d], o);
@@ -478,7 +408,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
             }
             if (PHYS == ASTRO_RMHD) {
                 const double* q = a.prk;
-                const double psi = STAGE ? sD[I_PSI * T + tid] : q[8 * nc + cell];
+                const double psi = q[8 * nc + cell];
                 rhs[8] -= a.p.glm_cp * a.p.glm_cp * psi;
                 for (int rep = 0; rep < nres; ++rep) {
                     const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
@@ -487,7 +417,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
 #pragma unroll
                     for (int c = 5; c < 8; ++c) {
                         const double* B = q + (size_t)c * nc + cell;
-                        const double b0 = STAGE ? sD[(I_B + c - 5) * T + tid] : B[0];
+                        const double b0 = B[0];
                         double lap = (B[st[0]] - 2.0 * b0 + B[-st[0]]) * ix2 +
                                      (B[st[1]] - 2.0 * b0 + B[-st[1]]) * iy2 +
                                      (B[st[2]] - 2.0 * b0 + B[-st[2]]) * iz2;
@@ -528,7 +458,6 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                 }
             }
         }
-        if constexpr (STAGE) cp_async_wait_all();
         if (a.rhs_only) {
 #pragma unroll
             for (int v = 0; v < NM; ++v) a.dst[(size_t)v * nc + cell] = rhs[v];
@@ -537,7 +466,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
             const Phys<double> P = Phys<double>::from(a.p);
             double q0[NM], U0[NM], Un[NM], q[NM];
 #pragma unroll
-            for (int v = 0; v < NM; ++v) q0[v] = STAGE ? sD[v * T + tid] : a.pr0[(size_t)v * nc + cell];
+            for (int v = 0; v < NM; ++v) q0[v] = a.pr0[(size_t)v * nc + cell];
             if (PHYS == ASTRO_SRHD) s_p2c(P, q0, U0);
             else r_p2c(P, q0, U0);
             const double dt = a.dt;
@@ -547,7 +476,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                 double un;
                 if (a.stage == 0) un = __dadd_rn(u0, __dmul_rn(dt, r));
                 else {
-                    const double uk = STAGE ? sD[(I_U + v) * T + tid] : a.U[(size_t)v * nc + cell];
+                    const double uk = a.U[(size_t)v * nc + cell];
                     if (a.nstages == 2)
                         un = __dmul_rn(0.5, __dadd_rn(__dadd_rn(u0, uk), __dmul_rn(dt, r)));
                     else if (a.stage == 1)
@@ -576,10 +505,10 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : (DEFER ? 4 : 6)) k
                 const int t = v - po;
                 if (np > 0 && t >= 0 && t < np) {
                     const size_t o = (size_t)v * nc + cell;
-                    const double t0 = STAGE ? sD[(I_T0 + t) * T + tid] : a.pr0[o], r = rp[t];
+                    const double t0 = a.pr0[o], r = rp[t];
                     if (a.stage == 0) out = __dadd_rn(t0, __dmul_rn(dt, r));
                     else {
-                        const double tk = STAGE ? sD[(I_TK + t) * T + tid] : a.prk[o];
+                        const double tk = a.prk[o];
                         if (a.nstages == 2)
                             out = __dmul_rn(0.5, __dadd_rn(__dadd_rn(t0, tk), __dmul_rn(dt, r)));
                         else if (a.stage == 1)
@@ -894,26 +823,9 @@ cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-// one update launch; the staged (DEFER) variants take dynamic shared memory,
-// whose per-kernel limit is raised once to the largest size they can ask for
 template <int PH, typename RF, bool DEF, bool PAS>
 void launch_update_t(const UpdArgs& a, dim3 grd, dim3 blk, cudaStream_t s) {
-    constexpr int nm = PH == ASTRO_SRHD ? 5 : 9;
-    size_t smem = 0;
-    if (DEF) {
-        static bool attr[64] = {};
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (dev < 0 || dev >= 64 || !attr[dev]) {
-            cudaFuncSetAttribute(k_update<PH, RF, DEF, PAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)update_smem_bytes(nm, sizeof(RF), kMaxPassive));
-            cudaFuncSetAttribute(k_update<PH, RF, DEF, PAS>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                 cudaSharedmemCarveoutMaxShared);
-            if (dev >= 0 && dev < 64) attr[dev] = true;
-        }
-        smem = update_smem_bytes(nm, sizeof(RF), a.p.n_passive);
-    }
-    k_update<PH, RF, DEF, PAS><<<grd, blk, smem, s>>>(a);
+    k_update<PH, RF, DEF, PAS><<<grd, blk, 0, s>>>(a);
 }
 
 cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
