@@ -863,7 +863,7 @@ cudaError_t face_passes(const AstroParams& p, const AstroGrid& g, const Bounds& 
     if (mixed && !prf_ready) {
         const size_t n = (size_t)(p.physics == ASTRO_SRHD ? 5 : 9) * g.nx * g.ny * g.nz;
         k_prim_f32<<<sm_count_cached() * 8, 256, 0, s>>>(pr, prf, n);
-        mark(0, s);
+        mark(2, s);
     }
     for (int oi = 0; oi < 3; ++oi) {
         const int d = order[oi];
