@@ -56,6 +56,19 @@ class AstroNozzle(C.Structure):
                 ("b_amb_x", C.c_double)]
 
 
+class AstroChemistry(C.Structure):
+    _fields_ = [("ng", C.c_int32), ("chem_offset", C.c_int32), ("x", C.c_double),
+                ("y", C.c_double), ("tunit_k", C.c_double), ("rate_scale", C.c_double),
+                ("energy_scale", C.c_double), ("tmin_k", C.c_double), ("gamma", C.c_double)]
+
+
+class AstroDissipation(C.Structure):
+    _fields_ = [("ng", C.c_int32), ("advect", C.c_int32), ("zeta", C.c_double),
+                ("eta", C.c_double), ("kappa", C.c_double), ("tau_bulk", C.c_double),
+                ("tau_shear", C.c_double), ("tau_heat", C.c_double), ("cap_frac", C.c_double),
+                ("p_max", C.c_double)]
+
+
 class AstroC2PStats(C.Structure):
     _fields_ = [(n, C.c_ulonglong) for n in
                 ("cells", "newton", "bisection", "hydro_fallback", "learned_polish",
@@ -90,6 +103,11 @@ PROTOS = {
     "astro_periodic_yz": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
     "astro_outflow_right_x": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
     "astro_outflow_yz": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
+    "astro_ion_chemistry": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroChemistry),
+                                      C.c_double, _VP]),
+    "astro_causal_dissipation_workspace_bytes": (C.c_size_t, [C.POINTER(AstroGrid)]),
+    "astro_causal_dissipation": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroDissipation),
+                                           C.c_double, _VP, C.c_size_t, _VP]),
     "astro_nozzle_left_x": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroNozzle),
                                       _DP, _VP, C.c_int32, _VP]),
     "astro_p2c": (C.c_int, [C.POINTER(AstroParams), _DP, _DP, C.c_int64, _VP]),

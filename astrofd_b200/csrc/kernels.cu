@@ -1172,6 +1172,143 @@ __global__ void k_two_temperature(double* pr, int nx, int ny, int nz, int ng, do
     }
 }
 
+// H/He ionisation (core/chemistry.py:43-139): rates are the reference's
+// fits; operation order follows its expressions
+__device__ __forceinline__ double chem_clamp(double x, double lo, double hi) {
+    return x < lo ? lo : (x > hi ? hi : x);
+}
+__device__ __forceinline__ double chem_ci(double a, double e, double T) {
+    return a * sqrt(T) * exp(-e / rmax(T, 1.0)) / (1.0 + sqrt(T / 1.0e5));
+}
+
+__global__ void k_ion_chemistry(double* pr, int nx, int ny, int nz, AstroChemistry c, double dt) {
+    const double SMALL = 1e-20;
+    const size_t nc = (size_t)nx * ny * nz;
+    const int ng = c.ng, ex = nx - 2 * ng, ey = ny - 2 * ng, ez = nz - 2 * ng;
+    const size_t n = (size_t)ex * ey * ez;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = ng + (int)(t % ez), j = ng + (int)((t / ez) % ey), i = ng + (int)(t / ((size_t)ez * ey));
+        const size_t cl = ((size_t)i * ny + j) * nz + k;
+        const double rho = pr[cl], p = pr[4 * nc + cl];
+        if (!(rho > 0.0) || !(p > 0.0)) continue;
+        double T = (p / rmax(rho, SMALL)) * c.tunit_k;
+        if (T < c.tmin_k) T = c.tmin_k;
+        const double nH = c.x * rho, nHe = c.y * rho / 4.0;
+        double* s = pr + (size_t)c.chem_offset * nc + cl;
+        const double xHII = chem_clamp(s[0], 0.0, 1.0);
+        double xHeII = chem_clamp(s[nc], 0.0, 1.0);
+        const double xHeIII = chem_clamp(s[2 * nc], 0.0, 1.0);
+        xHeII = rmin(xHeII, 1.0 - xHeIII);
+        const double xHeI = rmax(0.0, 1.0 - xHeII - xHeIII);
+        const double xHI = 1.0 - xHII;
+        const double ne = rmax(nH * xHII + nHe * (xHeII + 2.0 * xHeIII), SMALL);
+        const double C_H = c.rate_scale * chem_ci(5.85e-11, 157809.1, T);
+        const double C_HeI = c.rate_scale * chem_ci(2.38e-11, 285335.4, T);
+        const double C_HeII = c.rate_scale * chem_ci(5.68e-12, 631515.0, T);
+        const double A_H = c.rate_scale * (2.59e-13 * pow(T / 1.0e4, -0.7));
+        const double A_HeII = c.rate_scale * (1.50e-10 * pow(T / 1.0e4, -0.6353));
+        const double A_HeIII = c.rate_scale * (3.36e-10 * pow(T / 1.0e4, -0.5));
+        double xHII_n = (xHII + dt * ne * C_H * xHI) / (1.0 + dt * ne * A_H);
+        const double xHeIII_n =
+            chem_clamp((xHeIII + dt * ne * C_HeII * xHeII) / (1.0 + dt * ne * A_HeIII), 0.0, 1.0);
+        double xHeII_n = (xHeII + dt * ne * (C_HeI * xHeI + A_HeIII * xHeIII_n)) /
+                         (1.0 + dt * ne * (A_HeII + C_HeII));
+        xHII_n = chem_clamp(xHII_n, 0.0, 1.0);
+        xHeII_n = chem_clamp(xHeII_n, 0.0, 1.0 - xHeIII_n);
+        const double dE = c.energy_scale * (nH * 157809.1 * (xHII_n - xHII) +
+                                            nHe * 285335.4 * (xHeII_n - xHeII) +
+                                            nHe * 631515.0 * (xHeIII_n - xHeIII));
+        double pn = p + (-(c.gamma - 1.0) * dE / rmax(c.tunit_k, SMALL));
+        if (pn < SMALL) pn = SMALL;
+        pr[4 * nc + cl] = pn;
+        s[0] = xHII_n;
+        s[nc] = xHeII_n;
+        s[2 * nc] = xHeIII_n;
+    }
+}
+
+// Causal dissipation (core/dissipation.py:5-215), interior cells.  Pass 1:
+// first-order upwind advection of the 10 dissipative variables from the old
+// values into scratch (the reference's copies).  Pass 2: relaxation from the
+// advected values (or pr without advection), writing all 10 back.
+__global__ void k_dissip_advect(const double* pr, double* adv, int nx, int ny, int nz, int ng,
+                                double dt, double dx, double dy, double dz) {
+    const size_t nc = (size_t)nx * ny * nz;
+    const int ex = nx - 2 * ng, ey = ny - 2 * ng, ez = nz - 2 * ng;
+    const size_t n = (size_t)ex * ey * ez;
+    const long sx = (long)ny * nz, sy = nz;
+    const double hx = rmax(dx, 1e-12), hy = rmax(dy, 1e-12), hz = rmax(dz, 1e-12);
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = ng + (int)(t % ez), j = ng + (int)((t / ez) % ey), i = ng + (int)(t / ((size_t)ez * ey));
+        const size_t c = ((size_t)i * ny + j) * nz + k;
+        const double vx = pr[nc + c], vy = pr[2 * nc + c], vz = pr[3 * nc + c];
+        for (int v = 0; v < 10; ++v) {
+            const double* a = pr + (size_t)(5 + v) * nc + c;
+            const double u0 = a[0];
+            const double ddx = vx > 0.0 ? (u0 - a[-sx]) / hx : (a[sx] - u0) / hx;
+            const double ddy = vy > 0.0 ? (u0 - a[-sy]) / hy : (a[sy] - u0) / hy;
+            const double ddz = vz > 0.0 ? (u0 - a[-1]) / hz : (a[1] - u0) / hz;
+            adv[(size_t)v * nc + c] = u0 - dt * (vx * ddx + vy * ddy + vz * ddz);
+        }
+    }
+}
+
+__device__ __forceinline__ double dcap(double x, double cap) {
+    return x > cap ? cap : (x < -cap ? -cap : x);
+}
+
+__global__ void k_dissip_relax(double* pr, const double* adv, int nx, int ny, int nz,
+                               AstroDissipation c, double dt, double dx, double dy, double dz) {
+    const size_t nc = (size_t)nx * ny * nz;
+    const int ng = c.ng, ex = nx - 2 * ng, ey = ny - 2 * ng, ez = nz - 2 * ng;
+    const size_t n = (size_t)ex * ey * ez;
+    const long sx = (long)ny * nz, sy = nz;
+    const double i2x = 0.5 / rmax(dx, 1e-12), i2y = 0.5 / rmax(dy, 1e-12), i2z = 0.5 / rmax(dz, 1e-12);
+    const double cap = c.cap_frac * c.p_max;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+         t += (size_t)gridDim.x * blockDim.x) {
+        const int k = ng + (int)(t % ez), j = ng + (int)((t / ez) % ey), i = ng + (int)(t / ((size_t)ez * ey));
+        const size_t cl = ((size_t)i * ny + j) * nz + k;
+        double d[10];
+        for (int v = 0; v < 10; ++v) d[v] = adv ? adv[(size_t)v * nc + cl] : pr[(size_t)(5 + v) * nc + cl];
+        auto g = [&](int var, long off) { return pr[(size_t)var * nc + cl + off]; };
+        const double dvx_dx = (g(1, sx) - g(1, -sx)) * i2x, dvx_dy = (g(1, sy) - g(1, -sy)) * i2y,
+                     dvx_dz = (g(1, 1) - g(1, -1)) * i2z;
+        const double dvy_dx = (g(2, sx) - g(2, -sx)) * i2x, dvy_dy = (g(2, sy) - g(2, -sy)) * i2y,
+                     dvy_dz = (g(2, 1) - g(2, -1)) * i2z;
+        const double dvz_dx = (g(3, sx) - g(3, -sx)) * i2x, dvz_dy = (g(3, sy) - g(3, -sy)) * i2y,
+                     dvz_dz = (g(3, 1) - g(3, -1)) * i2z;
+        const double divv = dvx_dx + dvy_dy + dvz_dz;
+        if (c.zeta != 0.0) {
+            const double pi_eq = -c.zeta * divv;
+            d[0] = dcap((d[0] + dt * pi_eq / c.tau_bulk) / (1.0 + dt / c.tau_bulk), cap);
+        }
+        if (c.eta != 0.0) {
+            const double sxx = dvx_dx - (1.0 / 3.0) * divv, syy = dvy_dy - (1.0 / 3.0) * divv;
+            const double szz = dvz_dz - (1.0 / 3.0) * divv;
+            const double sxy = 0.5 * (dvx_dy + dvy_dx), sxz = 0.5 * (dvx_dz + dvz_dx);
+            const double syz = 0.5 * (dvy_dz + dvz_dy);
+            const double e2 = -2.0 * c.eta, ts = c.tau_shear;
+            const double eq[6] = {e2 * sxx, e2 * syy, e2 * szz, e2 * sxy, e2 * sxz, e2 * syz};
+            double s6[6];
+            for (int m = 0; m < 6; ++m) s6[m] = (d[1 + m] + dt * eq[m] / ts) / (1.0 + dt / ts);
+            s6[2] = -(s6[0] + s6[1]);  // traceless
+            for (int m = 0; m < 6; ++m) d[1 + m] = dcap(s6[m], cap);
+        }
+        if (c.kappa != 0.0) {
+            auto T = [&](long off) { return g(4, off) / rmax(g(0, off), 1e-12); };
+            const double dTdx = (T(sx) - T(-sx)) * i2x, dTdy = (T(sy) - T(-sy)) * i2y,
+                         dTdz = (T(1) - T(-1)) * i2z;
+            const double eq[3] = {-c.kappa * dTdx, -c.kappa * dTdy, -c.kappa * dTdz};
+            for (int m = 0; m < 3; ++m)
+                d[7 + m] = dcap((d[7 + m] + dt * eq[m] / c.tau_heat) / (1.0 + dt / c.tau_heat), cap);
+        }
+        for (int v = 0; v < 10; ++v) pr[(size_t)(5 + v) * nc + cl] = d[v];
+    }
+}
+
 int grid_for(size_t n, int block) {
     size_t g = (n + block - 1) / block;
     if (g > 148 * 32) g = 148 * 32;
@@ -1447,6 +1584,45 @@ int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, dou
     k_two_temperature<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(
         pr, g->nx, g->ny, g->nz, ng, dt, tau, thermo_offset);
     mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_ion_chemistry(double* pr, const AstroGrid* g, const AstroChemistry* c, double dt,
+                        void* stream) {
+    if (!pr || !g || !c || c->ng < 0 || c->chem_offset < 5) return ASTRO_E_INVALID;
+    if (g->nv < c->chem_offset + 3) return ASTRO_E_SHAPE;
+    if (g->nx <= 2 * c->ng || g->ny <= 2 * c->ng || g->nz <= 2 * c->ng) return ASTRO_OK;
+    const size_t n = (size_t)(g->nx - 2 * c->ng) * (g->ny - 2 * c->ng) * (g->nz - 2 * c->ng);
+    k_ion_chemistry<<<grid_for(n, 128), 128, 0, (cudaStream_t)stream>>>(pr, g->nx, g->ny, g->nz,
+                                                                        *c, dt);
+    mark(2, (cudaStream_t)stream);
+    return cuda_status(cudaGetLastError());
+}
+
+size_t astro_causal_dissipation_workspace_bytes(const AstroGrid* g) {
+    if (!g || g->nx < 1 || g->ny < 1 || g->nz < 1) return 0;
+    return (size_t)10 * g->nx * g->ny * g->nz * sizeof(double);
+}
+
+int astro_causal_dissipation(double* pr, const AstroGrid* g, const AstroDissipation* c, double dt,
+                             void* work, size_t work_bytes, void* stream) {
+    if (!pr || !g || !c || c->ng < 1) return ASTRO_E_INVALID;
+    if (g->nv < 15) return ASTRO_E_SHAPE;
+    if (c->tau_bulk <= 0.0 || c->tau_shear <= 0.0 || c->tau_heat <= 0.0) return ASTRO_E_INVALID;
+    if (g->nx <= 2 * c->ng || g->ny <= 2 * c->ng || g->nz <= 2 * c->ng) return ASTRO_OK;
+    if (c->advect && (!work || work_bytes < astro_causal_dissipation_workspace_bytes(g)))
+        return ASTRO_E_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t n = (size_t)(g->nx - 2 * c->ng) * (g->ny - 2 * c->ng) * (g->nz - 2 * c->ng);
+    double* adv = c->advect ? (double*)work : nullptr;
+    if (adv) {
+        k_dissip_advect<<<grid_for(n, 128), 128, 0, s>>>(pr, adv, g->nx, g->ny, g->nz, c->ng, dt,
+                                                         g->dx, g->dy, g->dz);
+        mark(2, s);
+    }
+    k_dissip_relax<<<grid_for(n, 128), 128, 0, s>>>(pr, adv, g->nx, g->ny, g->nz, *c, dt, g->dx,
+                                                    g->dy, g->dz);
+    mark(2, s);
     return cuda_status(cudaGetLastError());
 }
 

@@ -258,6 +258,33 @@ int astro_cooling_heating(double* pr, const AstroGrid* g, int ng, double dt, dou
 int astro_two_temperature(double* pr, const AstroGrid* g, int ng, double dt, double tau,
                           int thermo_offset, void* stream);
 
+/* H/He non-equilibrium ionisation on the interior cells, in place: replaces
+ * chemistry.apply_ion_chemistry (core/chemistry.py:43).  Species xHII, xHeII,
+ * xHeIII at variables chem_offset.. chem_offset+2; implicit recombination,
+ * explicit ionisation, the ionisation energy taken from the pressure. */
+typedef struct AstroChemistry {
+    int32_t ng, chem_offset;
+    double x, y;                 /* hydrogen / helium mass fractions         */
+    double tunit_k, rate_scale, energy_scale, tmin_k, gamma;
+} AstroChemistry;
+int astro_ion_chemistry(double* pr, const AstroGrid* g, const AstroChemistry* c, double dt,
+                        void* stream);
+
+/* Israel-Stewart causal dissipation of the 15-variable SRHD block, in place:
+ * replaces dissipation.apply_causal_dissipation (core/dissipation.py:5).  With
+ * advect, first-order upwind advection of pi, pi_ij, q_i (variables 5..14) by
+ * the velocity, then relaxation toward the Navier-Stokes targets of bulk
+ * (zeta != 0), shear (eta != 0) and heat flux (kappa != 0) with the given
+ * relaxation times, capped at cap_frac * p_max.  Scratch:
+ * astro_causal_dissipation_workspace_bytes(g) bytes (10 float64 per cell). */
+typedef struct AstroDissipation {
+    int32_t ng, advect;
+    double zeta, eta, kappa, tau_bulk, tau_shear, tau_heat, cap_frac, p_max;
+} AstroDissipation;
+size_t astro_causal_dissipation_workspace_bytes(const AstroGrid* g);
+int astro_causal_dissipation(double* pr, const AstroGrid* g, const AstroDissipation* c, double dt,
+                             void* work, size_t work_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

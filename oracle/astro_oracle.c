@@ -1260,3 +1260,142 @@ int oracle_num_threads(void) {
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------ */
+/* H/He ionisation (chemistry.py:43-139), interior cells, in place      */
+/* ------------------------------------------------------------------ */
+static double ch_clamp(double x, double lo, double hi) {
+    if (x < lo) return lo;
+    if (x > hi) return hi;
+    return x;
+}
+static double ch_ci(double a, double e, double T) {
+    return a * sqrt(T) * exp(-e / dmax(T, 1.0)) / (1.0 + sqrt(T / 1.0e5));
+}
+void oracle_ion_chemistry(double* pr, int nv, int nx, int ny, int nz, int ng, int off, double dt,
+                          double X, double Y, double tunit, double rate_scale,
+                          double energy_scale, double tmin, double gamma) {
+    OGrid g0 = {nv, nx, ny, nz};
+    const OGrid* g = &g0;
+    const double CSMALL = 1e-20; /* chemistry.py's SMALL */
+    for (int i = ng; i < nx - ng; ++i)
+        for (int j = ng; j < ny - ng; ++j)
+            for (int k = ng; k < nz - ng; ++k) {
+                double rho = P(0, i, j, k), p = P(4, i, j, k);
+                if (rho <= 0.0 || p <= 0.0) continue;
+                double T = (p / dmax(rho, CSMALL)) * tunit;
+                if (T < tmin) T = tmin;
+                double nH = X * rho, nHe = Y * rho / 4.0;
+                double xHII = ch_clamp(P(off, i, j, k), 0.0, 1.0);
+                double xHeII = ch_clamp(P(off + 1, i, j, k), 0.0, 1.0);
+                double xHeIII = ch_clamp(P(off + 2, i, j, k), 0.0, 1.0);
+                xHeII = xHeII < 1.0 - xHeIII ? xHeII : 1.0 - xHeIII;
+                double xHeI = dmax(0.0, 1.0 - xHeII - xHeIII);
+                double xHI = 1.0 - xHII;
+                double ne = dmax(nH * xHII + nHe * (xHeII + 2.0 * xHeIII), CSMALL);
+                double C_H = rate_scale * ch_ci(5.85e-11, 157809.1, T);
+                double C_HeI = rate_scale * ch_ci(2.38e-11, 285335.4, T);
+                double C_HeII = rate_scale * ch_ci(5.68e-12, 631515.0, T);
+                double A_H = rate_scale * (2.59e-13 * pow(T / 1.0e4, -0.7));
+                double A_HeII = rate_scale * (1.50e-10 * pow(T / 1.0e4, -0.6353));
+                double A_HeIII = rate_scale * (3.36e-10 * pow(T / 1.0e4, -0.5));
+                double xHII_n = (xHII + dt * ne * C_H * xHI) / (1.0 + dt * ne * A_H);
+                double xHeIII_n = ch_clamp((xHeIII + dt * ne * C_HeII * xHeII) / (1.0 + dt * ne * A_HeIII),
+                                           0.0, 1.0);
+                double xHeII_n = (xHeII + dt * ne * (C_HeI * xHeI + A_HeIII * xHeIII_n)) /
+                                 (1.0 + dt * ne * (A_HeII + C_HeII));
+                xHII_n = ch_clamp(xHII_n, 0.0, 1.0);
+                xHeII_n = ch_clamp(xHeII_n, 0.0, 1.0 - xHeIII_n);
+                double dE = energy_scale * (nH * 157809.1 * (xHII_n - xHII) +
+                                            nHe * 285335.4 * (xHeII_n - xHeII) +
+                                            nHe * 631515.0 * (xHeIII_n - xHeIII));
+                double pn = p + (-(gamma - 1.0) * dE / dmax(tunit, CSMALL));
+                if (pn < CSMALL) pn = CSMALL;
+                P(4, i, j, k) = pn;
+                P(off, i, j, k) = xHII_n;
+                P(off + 1, i, j, k) = xHeII_n;
+                P(off + 2, i, j, k) = xHeIII_n;
+            }
+}
+
+/* ------------------------------------------------------------------ */
+/* causal dissipation (dissipation.py:5-215), interior cells, in place; */
+/* work: 10 * nx*ny*nz doubles (the reference's advected copies)        */
+/* ------------------------------------------------------------------ */
+static double ocap(double x, double cap) {
+    if (x > cap) return cap;
+    if (x < -cap) return -cap;
+    return x;
+}
+void oracle_causal_dissipation(double* pr, int nv, int nx, int ny, int nz, int ng, double dt,
+                               double dx, double dy, double dz, double zeta, double eta,
+                               double kappa, double tau_bulk, double tau_shear, double tau_heat,
+                               double cap_frac, double pmax, int advect, double* work) {
+    OGrid g0 = {nv, nx, ny, nz};
+    const OGrid* g = &g0;
+    const size_t nc = (size_t)nx * ny * nz;
+    const double hx = dmax(dx, 1e-12), hy = dmax(dy, 1e-12), hz = dmax(dz, 1e-12);
+    if (advect) {
+        memcpy(work, pr + 5 * nc, 10 * nc * sizeof(double));
+        for (int i = ng; i < nx - ng; ++i)
+            for (int j = ng; j < ny - ng; ++j)
+                for (int k = ng; k < nz - ng; ++k) {
+                    double vx = P(1, i, j, k), vy = P(2, i, j, k), vz = P(3, i, j, k);
+                    for (int v = 5; v < 15; ++v) {
+                        double u0 = P(v, i, j, k), ddx, ddy, ddz;
+                        if (vx > 0.0) ddx = (u0 - P(v, i - 1, j, k)) / hx;
+                        else ddx = (P(v, i + 1, j, k) - u0) / hx;
+                        if (vy > 0.0) ddy = (u0 - P(v, i, j - 1, k)) / hy;
+                        else ddy = (P(v, i, j + 1, k) - u0) / hy;
+                        if (vz > 0.0) ddz = (u0 - P(v, i, j, k - 1)) / hz;
+                        else ddz = (P(v, i, j, k + 1) - u0) / hz;
+                        work[(size_t)(v - 5) * nc + ((size_t)i * ny + j) * nz + k] =
+                            u0 - dt * (vx * ddx + vy * ddy + vz * ddz);
+                    }
+                }
+        memcpy(pr + 5 * nc, work, 10 * nc * sizeof(double));
+    }
+    const double i2x = 0.5 / hx, i2y = 0.5 / hy, i2z = 0.5 / hz, cap = cap_frac * pmax;
+    for (int i = ng; i < nx - ng; ++i)
+        for (int j = ng; j < ny - ng; ++j)
+            for (int k = ng; k < nz - ng; ++k) {
+                double dvx_dx = (P(1, i + 1, j, k) - P(1, i - 1, j, k)) * i2x;
+                double dvx_dy = (P(1, i, j + 1, k) - P(1, i, j - 1, k)) * i2y;
+                double dvx_dz = (P(1, i, j, k + 1) - P(1, i, j, k - 1)) * i2z;
+                double dvy_dx = (P(2, i + 1, j, k) - P(2, i - 1, j, k)) * i2x;
+                double dvy_dy = (P(2, i, j + 1, k) - P(2, i, j - 1, k)) * i2y;
+                double dvy_dz = (P(2, i, j, k + 1) - P(2, i, j, k - 1)) * i2z;
+                double dvz_dx = (P(3, i + 1, j, k) - P(3, i - 1, j, k)) * i2x;
+                double dvz_dy = (P(3, i, j + 1, k) - P(3, i, j - 1, k)) * i2y;
+                double dvz_dz = (P(3, i, j, k + 1) - P(3, i, j, k - 1)) * i2z;
+                double divv = dvx_dx + dvy_dy + dvz_dz;
+                if (zeta != 0.0) {
+                    double pi_eq = -zeta * divv;
+                    P(5, i, j, k) = ocap((P(5, i, j, k) + dt * pi_eq / tau_bulk) / (1.0 + dt / tau_bulk), cap);
+                }
+                if (eta != 0.0) {
+                    double sxx = dvx_dx - (1.0 / 3.0) * divv, syy = dvy_dy - (1.0 / 3.0) * divv;
+                    double szz = dvz_dz - (1.0 / 3.0) * divv;
+                    double sxy = 0.5 * (dvx_dy + dvy_dx), sxz = 0.5 * (dvx_dz + dvz_dx);
+                    double syz = 0.5 * (dvy_dz + dvz_dy);
+                    double eq[6] = {-2.0 * eta * sxx, -2.0 * eta * syy, -2.0 * eta * szz,
+                                    -2.0 * eta * sxy, -2.0 * eta * sxz, -2.0 * eta * syz};
+                    double s6[6];
+                    for (int m = 0; m < 6; ++m)
+                        s6[m] = (P(6 + m, i, j, k) + dt * eq[m] / tau_shear) / (1.0 + dt / tau_shear);
+                    s6[2] = -(s6[0] + s6[1]);
+                    for (int m = 0; m < 6; ++m) P(6 + m, i, j, k) = ocap(s6[m], cap);
+                }
+                if (kappa != 0.0) {
+#define OT(a, b, c) (P(4, a, b, c) / dmax(P(0, a, b, c), 1e-12))
+                    double dTdx = (OT(i + 1, j, k) - OT(i - 1, j, k)) * i2x;
+                    double dTdy = (OT(i, j + 1, k) - OT(i, j - 1, k)) * i2y;
+                    double dTdz = (OT(i, j, k + 1) - OT(i, j, k - 1)) * i2z;
+#undef OT
+                    double eq[3] = {-kappa * dTdx, -kappa * dTdy, -kappa * dTdz};
+                    for (int m = 0; m < 3; ++m)
+                        P(12 + m, i, j, k) = ocap((P(12 + m, i, j, k) + dt * eq[m] / tau_heat) /
+                                                  (1.0 + dt / tau_heat), cap);
+                }
+            }
+}

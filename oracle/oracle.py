@@ -74,6 +74,9 @@ def lib():
                                            C.c_double, C.c_double,
                                            C.POINTER(ONozzle), dp]
         L.oracle_nozzle_left_x.restype = C.c_long
+        L.oracle_ion_chemistry.argtypes = [dp] + [C.c_int] * 6 + [C.c_double] * 8
+        L.oracle_causal_dissipation.argtypes = ([dp] + [C.c_int] * 5 + [C.c_double] * 12 +
+                                                [C.c_int, dp])
         L.oracle_cooling.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                      C.c_double, C.c_double, C.c_double, C.c_double]
         L.oracle_two_temperature.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -252,6 +255,51 @@ def apply_nozzle_left_x(pr, dx, dy, dz, ny_loc, nz_loc, y0, z0, rng, cfg):
     used = lib().oracle_nozzle_left_x(_dp(pr), *pr.shape, dy, dz, ny_loc, nz_loc, y0, z0,
                                       C.byref(c), _dp(rnd))
     assert used == n, (used, n)
+
+
+def apply_ion_chemistry(pr, dt, cfg):
+    """chemistry.apply_ion_chemistry (core/chemistry.py:43), with its gating."""
+    if not cfg.get("CHEMISTRY_ENABLED", False) or int(cfg.get("N_CHEM", 0)) < 3:
+        return pr
+    off = int(cfg.get("CHEM_OFFSET", 0))
+    if pr.shape[0] <= off + 2:
+        return pr
+    assert pr.flags.c_contiguous and pr.dtype == np.float64
+    lib().oracle_ion_chemistry(_dp(pr), *pr.shape, int(cfg.get("NG", 2)), off, float(dt),
+                               float(cfg.get("CHEM_X", 0.76)), float(cfg.get("CHEM_Y", 0.24)),
+                               float(cfg.get("CHEM_TUNIT_K", 1.0e4)),
+                               float(cfg.get("CHEM_RATE_SCALE", 1.0)),
+                               float(cfg.get("CHEM_ENERGY_SCALE", 1.0)),
+                               float(cfg.get("CHEM_TMIN_K", 1.0)),
+                               float(cfg.get("GAMMA", 5.0 / 3.0)))
+    return pr
+
+
+def dissipation_taus(cfg):
+    """The reference's relaxation times: a per-channel key, else RELAX_TAU
+    (a zero per-channel value also falls back), core/dissipation.py:18-20."""
+    base = cfg.get("RELAX_TAU", 0.1)
+    return tuple(float(cfg.get(k, base) or base)
+                 for k in ("RELAX_TAU_BULK", "RELAX_TAU_SHEAR", "RELAX_TAU_HEAT"))
+
+
+def apply_causal_dissipation(pr, dt, dx, dy, dz, cfg):
+    """dissipation.apply_causal_dissipation (core/dissipation.py:5)."""
+    if not cfg.get("DISSIPATION_ENABLED", False) or cfg.get("PHYSICS") not in ("hydro", "grhd"):
+        return pr
+    zeta, eta, kappa = (float(cfg.get(k, 0.0)) for k in ("BULK_ZETA", "SHEAR_ETA", "HEAT_KAPPA"))
+    tb, ts, th = dissipation_taus(cfg)
+    if (zeta == 0.0 and eta == 0.0 and kappa == 0.0) or min(tb, ts, th) <= 0.0 or pr.shape[0] < 15:
+        return pr
+    assert pr.flags.c_contiguous and pr.dtype == np.float64
+    work = np.empty((10,) + pr.shape[1:])
+    lib().oracle_causal_dissipation(_dp(pr), *pr.shape, int(cfg.get("NG", 2)), float(dt),
+                                    float(dx), float(dy), float(dz), zeta, eta, kappa, tb, ts, th,
+                                    float(cfg.get("DISSIPATION_CAP_FRAC", 0.5)),
+                                    float(cfg.get("P_MAX", 1.0)),
+                                    1 if bool(cfg.get("DISSIPATION_ADVECT", True)) else 0,
+                                    _dp(work))
+    return pr
 
 
 def apply_cooling_heating(pr, dt, cfg):

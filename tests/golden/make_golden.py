@@ -27,7 +27,8 @@ from cases import CASES, CASE_BY_NAME, DT_FRACTION  # noqa: E402
 import states  # noqa: E402
 
 SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
-           "c2p_rmhd", "c2p_srhd", "source_terms", "c1_run", "c5_run"]
+           "c2p_rmhd", "c2p_srhd", "source_terms", "c1_run", "c5_run", "chemistry",
+           "dissipation"]
 
 NOZZLE_BASE = dict(JET_RADIUS=0.1, SHEAR_THICK=0.02, NOZZLE_PROFILE="top_hat",
                    GAMMA_JET=7.088812050083354, ETA_RHO=0.1, P_EQ=0.01,
@@ -252,6 +253,49 @@ def run_loop(name, ref, out):
                             n=np.array(10), ng=np.array(3))
 
 
+def run_chem_dissip(name, ref, out):
+    """core/chemistry.py apply_ion_chemistry and core/dissipation.py
+    apply_causal_dissipation (plain Python in the reference) on seeded blocks."""
+    sys.path.insert(0, ref)
+    rng = np.random.default_rng(701 if name == "chemistry" else 702)
+    n, ng = 12, 2
+    N = n + 2 * ng
+    dt, d = 0.01, 1.0 / n
+    if name == "chemistry":
+        from core import chemistry as CH
+        pr = np.zeros((8, N, N, N))
+        pr[0] = 10.0 ** rng.uniform(-1, 1, (N, N, N))
+        pr[4] = pr[0] * 10.0 ** rng.uniform(-3, 2, (N, N, N))  # T = 10 K .. 1e6 K
+        pr[1:4] = 0.1 * rng.standard_normal((3, N, N, N))
+        pr[5:8] = rng.uniform(-0.1, 1.1, (3, N, N, N))          # clamps exercised
+        pr[0, 3, 3, 3] = -1.0                                    # skipped cell
+        outs = {}
+        for tag, scale in (("nominal", 1.0), ("fast", 1e9)):
+            cfg = dict(CHEMISTRY_ENABLED=True, N_CHEM=3, CHEM_OFFSET=5, NG=ng,
+                       CHEM_RATE_SCALE=scale, CHEM_ENERGY_SCALE=1e-6, GAMMA=5.0 / 3.0)
+            outs[tag] = CH.apply_ion_chemistry(pr.copy(), dt, cfg)
+            outs["cfg_" + tag] = np.array(json.dumps(cfg))
+        np.savez_compressed(out, pr_in=pr, dt=np.array(dt), **outs)
+    else:
+        from core import dissipation as DI
+        pr = np.zeros((15, N, N, N))
+        pr[0] = 1.0 + 0.5 * rng.random((N, N, N))
+        pr[4] = 0.1 + 0.5 * rng.random((N, N, N))
+        pr[1:4] = 0.3 * rng.standard_normal((3, N, N, N))
+        pr[5:15] = 0.2 * rng.standard_normal((10, N, N, N))
+        outs = {}
+        cases = {"full": dict(BULK_ZETA=0.1, SHEAR_ETA=0.05, HEAT_KAPPA=0.02, RELAX_TAU=0.1,
+                              RELAX_TAU_SHEAR=0.2, DISSIPATION_CAP_FRAC=0.5, P_MAX=0.5,
+                              DISSIPATION_ADVECT=True),
+                 "noadvect": dict(BULK_ZETA=0.0, SHEAR_ETA=0.3, HEAT_KAPPA=0.0, RELAX_TAU=0.05,
+                                  DISSIPATION_CAP_FRAC=0.5, P_MAX=1.0, DISSIPATION_ADVECT=False)}
+        for tag, extra in cases.items():
+            cfg = dict(DISSIPATION_ENABLED=True, PHYSICS="hydro", NG=ng, **extra)
+            outs[tag] = DI.apply_causal_dissipation(pr.copy(), dt, d, d, d, cfg)
+            outs["cfg_" + tag] = np.array(json.dumps(cfg))
+        np.savez_compressed(out, pr_in=pr, dt=np.array(dt), dx=np.array(d), **outs)
+
+
 def one(name, ref):
     out = os.path.join(HERE, name + ".npz")
     if name in CASE_BY_NAME:
@@ -262,6 +306,8 @@ def one(name, ref):
         run_c2p(name, ref, out)
     elif name == "source_terms":
         run_source(name, ref, out)
+    elif name in ("chemistry", "dissipation"):
+        run_chem_dissip(name, ref, out)
     else:
         run_loop(name, ref, out)
     print("wrote", out, flush=True)
