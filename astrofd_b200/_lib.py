@@ -105,6 +105,8 @@ PROTOS = {
     "astro_outflow_yz": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
     "astro_ion_chemistry": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroChemistry),
                                       C.c_double, _VP]),
+    "astro_diagnostics": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), C.c_int, _DP,
+                                    C.c_double, _DP, _VP]),
     "astro_causal_dissipation_workspace_bytes": (C.c_size_t, [C.POINTER(AstroGrid)]),
     "astro_causal_dissipation": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroDissipation),
                                            C.c_double, _VP, C.c_size_t, _VP]),

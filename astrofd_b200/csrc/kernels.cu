@@ -1309,6 +1309,68 @@ __global__ void k_dissip_relax(double* pr, const double* adv, int nx, int ny, in
     }
 }
 
+// run diagnostics (utils/diagnostics.py:5-57, 128-183)
+__device__ __forceinline__ void atomic_max_pos(double* dst, double v) {
+    // non-negative doubles order like their bit patterns
+    atomicMax((unsigned long long*)dst, (unsigned long long)__double_as_longlong(v));
+}
+
+__global__ void k_diagnostics(AstroParams p, const double* pr, int nv, int nx, int ny, int nz,
+                              int ng, double dx, double dy, double dz, double gamma,
+                              double* out) {
+    // cell counts below 2^31 (checked by the host), so 32-bit index arithmetic
+    const unsigned nc = (unsigned)nx * ny * nz;
+    const unsigned ey = ny - 2 * ng, ez = nz - 2 * ng;
+    const unsigned n = (unsigned)(nx - 2 * ng) * ey * ez;
+    const bool mhd = p.physics == ASTRO_RMHD, divb = nv >= 8;
+    double gmax = 0.0, sx = 0.0, bmax = 0.0, bsum = 0.0, bsq = 0.0, cnt = 0.0;
+    const int sX = ny * nz, sY = nz;
+    for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned k = ng + t % ez, j = ng + (t / ez) % ey, i = ng + t / (ez * ey);
+        const size_t c = ((size_t)i * ny + j) * nz + k;
+        const double vx = pr[nc + c], vy = pr[2 * nc + c], vz = pr[3 * nc + c];
+        double v2 = vx * vx + vy * vy + vz * vz;
+        if (v2 >= 1.0) v2 = 1.0 - 1e-14;
+        gmax = rmax(gmax, 1.0 / sqrt(1.0 - v2));
+        if (i == (unsigned)ng) {
+            double q[9], U[9];
+            for (int v = 0; v < (mhd ? 9 : 5); ++v) q[v] = pr[(size_t)v * nc + c];
+            Phys<double> P = Phys<double>::from(p);
+            P.gamma = P.srhd_gamma = gamma;
+            if (mhd) r_p2c(P, q, U);
+            else s_p2c(P, q, U);
+            sx += U[1];
+        }
+        if (divb) {
+            const double* B = pr + 5 * nc + c;
+            const double d = (B[sX] - B[-sX]) / (2.0 * dx) + (B[nc + sY] - B[nc - sY]) / (2.0 * dy) +
+                             (B[2 * nc + 1] - B[2 * nc - 1]) / (2.0 * dz);
+            bmax = rmax(bmax, fabs(d));
+            bsum += d;
+            bsq += d * d;
+            cnt += 1.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        gmax = rmax(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
+        bmax = rmax(bmax, __shfl_down_sync(0xffffffffu, bmax, o));
+        sx += __shfl_down_sync(0xffffffffu, sx, o);
+        bsum += __shfl_down_sync(0xffffffffu, bsum, o);
+        bsq += __shfl_down_sync(0xffffffffu, bsq, o);
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomic_max_pos(out, gmax);
+        if (sx != 0.0) atomicAdd(out + 1, sx);
+        if (divb) {
+            atomic_max_pos(out + 2, bmax);
+            atomicAdd(out + 3, bsum);
+            atomicAdd(out + 4, bsq);
+            atomicAdd(out + 5, cnt);
+        }
+    }
+}
+
 int grid_for(size_t n, int block) {
     size_t g = (n + block - 1) / block;
     if (g > 148 * 32) g = 148 * 32;
@@ -1622,6 +1684,22 @@ int astro_causal_dissipation(double* pr, const AstroGrid* g, const AstroDissipat
     }
     k_dissip_relax<<<grid_for(n, 128), 128, 0, s>>>(pr, adv, g->nx, g->ny, g->nz, *c, dt, g->dx,
                                                     g->dy, g->dz);
+    mark(2, s);
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_diagnostics(const AstroParams* p, const AstroGrid* g, int ng, const double* pr,
+                      double gamma, double* out, void* stream) {
+    if (!p || !g || !pr || !out || ng < 1) return ASTRO_E_INVALID;
+    if (g->nv < 5 || (p->physics == ASTRO_RMHD && g->nv < 9)) return ASTRO_E_SHAPE;
+    if ((double)g->nv * g->nx * g->ny * g->nz >= 2147483648.0) return ASTRO_E_SHAPE;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(out, 0, 6 * sizeof(double), s) != cudaSuccess) return ASTRO_E_CUDA;
+    if (g->nx <= 2 * ng || g->ny <= 2 * ng || g->nz <= 2 * ng) return ASTRO_OK;
+    const size_t n = (size_t)(g->nx - 2 * ng) * (g->ny - 2 * ng) * (g->nz - 2 * ng);
+    const int grid = grid_for(n, 256) < sm_count_cached() * 8 ? grid_for(n, 256) : sm_count_cached() * 8;
+    k_diagnostics<<<grid, 256, 0, s>>>(*p, pr, g->nv, g->nx, g->ny, g->nz, ng, g->dx, g->dy, g->dz,
+                                       gamma, out);
     mark(2, s);
     return cuda_status(cudaGetLastError());
 }

@@ -282,6 +282,19 @@ typedef struct AstroDissipation {
     double zeta, eta, kappa, tau_bulk, tau_shear, tau_heat, cap_frac, p_max;
 } AstroDissipation;
 size_t astro_causal_dissipation_workspace_bytes(const AstroGrid* g);
+
+/* --- run diagnostics (utils/diagnostics.py:5,128) -------------------------
+ * Device reductions over the interior of one block (ng ghost layers), into
+ * out[6] (device memory, overwritten): max Lorentz factor (v^2 capped below 1
+ * as the reference does), the sum of S_x = prim_to_cons(...)[1] over the first
+ * interior x layer with adiabatic index `gamma` (multiply by dy dz for the
+ * inlet flux; the reference passes no index there, so its module default 5/3
+ * applies whatever GAMMA is configured), and for blocks of 8+ variables
+ * max |div B|, the sum and the sum of squares of the central-difference div B
+ * and the cell count.  Sums are accumulated with atomics: their rounding
+ * depends on the order.  No reference counterpart for the MPI reductions. */
+int astro_diagnostics(const AstroParams* p, const AstroGrid* g, int ng, const double* pr,
+                      double gamma, double* out, void* stream);
 int astro_causal_dissipation(double* pr, const AstroGrid* g, const AstroDissipation* c, double dt,
                              void* work, size_t work_bytes, void* stream);
 

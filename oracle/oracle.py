@@ -320,5 +320,59 @@ def apply_two_temperature(pr, dt, cfg):
     return pr
 
 
+def diagnostics(pr, dx, dy, dz, ng, is_rmhd, v_max=0.999, p_max=1.0):
+    """One rank's diagnostics, restating utils/diagnostics.py: max Gamma
+    (:14-25) and the inlet flux accumulated cell by cell in (j, k) order
+    (:29-42) with prim_to_cons at its default adiabatic index 5/3; div B
+    (:141-160) with the reference's numpy max / sum over the (i, j, k)-ordered
+    values; the centreline (:72-99).  Dict of the values."""
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    inner = (slice(ng, pr.shape[1] - ng), slice(ng, pr.shape[2] - ng), slice(ng, pr.shape[3] - ng))
+    vx, vy, vz = (pr[v][inner] for v in (1, 2, 3))
+    v2 = vx * vx + vy * vy + vz * vz
+    v2 = np.where(v2 >= 1.0, 1.0 - 1e-14, v2)
+    out = dict(max_gamma=float(np.max(1.0 / np.sqrt(1.0 - v2))) if v2.size else 0.0)
+    nm = 9 if is_rmhd else 5
+    q = pr[:nm, ng, inner[1], inner[2]].reshape(nm, -1)
+    P = params_from_config("rmhd" if is_rmhd else "srhd",
+                           dict(GAMMA=5.0 / 3.0, V_MAX=v_max, P_MAX=p_max))
+    sx = p2c(P, q)[1]
+    flux = 0.0
+    for s in sx:
+        flux += s * dy * dz
+    out["inlet_flux"] = flux
+    out["inlet_sx"] = float(math.fsum(sx))
+    if pr.shape[0] >= 8:
+        i, j, k = inner
+        sh = lambda v, a, d: pr[v][tuple(slice(s.start + d, s.stop + d) if ax == a else s
+                                          for ax, s in enumerate(inner))]
+        d = ((sh(5, 0, 1) - sh(5, 0, -1)) / (2.0 * dx) + (sh(6, 1, 1) - sh(6, 1, -1)) / (2.0 * dy)
+             + (sh(7, 2, 1) - sh(7, 2, -1)) / (2.0 * dz)).ravel()
+        n = d.size
+        out.update(divb_max=float(np.max(np.abs(d))) if n else 0.0, divb_sum=float(np.sum(d)),
+                   divb_sumsq=float(np.sum(d * d)), divb_n=n)
+        out["divb_mean"] = out["divb_sum"] / n if n else 0.0
+        out["divb_rms"] = float(np.sqrt(out["divb_sumsq"] / n)) if n else 0.0
+    return out
+
+
+def centerline(pr, ng, v_max):
+    """(Gamma, rho, p, vx) of utils/diagnostics.py:72-99 for one rank."""
+    ny, nz = pr.shape[2] - 2 * ng, pr.shape[3] - 2 * ng
+    j, k = ng + ny // 2, ng + nz // 2
+    sl = slice(ng, pr.shape[1] - ng)
+    rho, vx, vy, vz, p = (pr[v, sl, j, k].copy() for v in range(5))
+    v2 = vx * vx + vy * vy + vz * vz
+    vmax2 = v_max * v_max
+    m = v2 >= vmax2
+    if np.any(m):
+        fac = v_max / np.sqrt(v2[m] + 1e-32)
+        vx[m] *= fac
+        vy[m] *= fac
+        vz[m] *= fac
+        v2[m] = vmax2 - 1e-14
+    return 1.0 / np.sqrt(1.0 - np.clip(v2, 0, 1 - 1e-14)), rho, p, vx
+
+
 def num_threads():
     return lib().oracle_num_threads()

@@ -28,7 +28,7 @@ import states  # noqa: E402
 
 SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
            "c2p_rmhd", "c2p_srhd", "source_terms", "c1_run", "c5_run", "chemistry",
-           "dissipation"]
+           "dissipation", "diagnostics"]
 
 NOZZLE_BASE = dict(JET_RADIUS=0.1, SHEAR_THICK=0.02, NOZZLE_PROFILE="top_hat",
                    GAMMA_JET=7.088812050083354, ETA_RHO=0.1, P_EQ=0.01,
@@ -296,6 +296,83 @@ def run_chem_dissip(name, ref, out):
         np.savez_compressed(out, pr_in=pr, dt=np.array(dt), dx=np.array(d), **outs)
 
 
+class _OneRank:
+    """The mpi4py surface utils/diagnostics.py uses, for one rank (mpi4py
+    is not installed where the fixtures are made)."""
+    MAX, SUM = "max", "sum"
+
+    def allreduce(self, v, op=None):
+        return v
+
+    def gather(self, v, root=0):
+        return [v]
+
+    def Gatherv(self, sendbuf, recvbuf, root=0):
+        recvbuf[0][:] = sendbuf
+
+
+def diagnostics_blocks():
+    """Seeded SRHD (5-variable) and RMHD (9-variable) blocks with cells at
+    v >= 1 (Gamma capping), above V_MAX on the centreline and at the inlet
+    (velocity cap of prim_to_cons_rmhd) and p above P_MAX."""
+    rng = np.random.default_rng(703)
+    n, ng = 10, 2
+    N = n + 2 * ng
+    out = {}
+    for name, nv in (("srhd", 5), ("rmhd", 9)):
+        pr = np.zeros((nv, N, N, N))
+        pr[0] = 0.5 + rng.random((N, N, N))
+        pr[4] = 10.0 ** rng.uniform(-3, 0.5, (N, N, N))
+        v = rng.standard_normal((3, N, N, N))
+        v *= rng.uniform(0.0, 0.995, (N, N, N)) / np.linalg.norm(v, axis=0)
+        pr[1:4] = v
+        pr[1:4, 4, 5, 6] *= 1.2 / np.linalg.norm(pr[1:4, 4, 5, 6])   # v > 1
+        pr[1:4, 5, 7, 7] *= 0.9995 / np.linalg.norm(pr[1:4, 5, 7, 7])  # centreline, > V_MAX
+        pr[1:4, ng, 3, 4] *= 0.9992 / np.linalg.norm(pr[1:4, ng, 3, 4])  # inlet, > V_MAX
+        if nv == 9:
+            pr[5:8] = 0.3 * rng.standard_normal((3, N, N, N))
+            pr[8] = 0.01 * rng.standard_normal((N, N, N))
+        out[name] = pr
+    return out, ng
+
+
+def run_diagnostics(name, ref, out):
+    """utils/diagnostics.py on one rank, with a stub communicator; the RMHD
+    block under GAMMA 4/3 (the diagnostics' prim_to_cons keeps 5/3)."""
+    import tempfile
+    import types
+    stub = types.ModuleType("mpi4py")
+    stub.MPI = _OneRank
+    sys.modules["mpi4py"] = stub
+    sys.path.insert(0, ref)
+    from core import srhd_core, rmhd_core
+    from utils import diagnostics as DG
+    cfg = dict(GAMMA=4.0 / 3.0, V_MAX=0.999, P_MAX=1.0)
+    rmhd_core.configure(cfg)
+    blocks, ng = diagnostics_blocks()
+    d = 0.1
+    rec = {}
+    for phys, pr in blocks.items():
+        with tempfile.TemporaryDirectory() as run:
+            comm = _OneRank()
+            rmhd = phys == "rmhd"
+            res = DG.compute_diagnostics_and_write(
+                pr, d, 0.7 * d, 1.3 * d, 0, None, comm, 0, 7, 0.25, 1e-3, 0.9, run,
+                rmhd_core.prim_to_cons_rmhd if rmhd else srhd_core.prim_to_cons, ng, rmhd)
+            DG.compute_centerline_and_write(pr, d, 0.7 * d, 1.3 * d, 0, None, comm, 0, 7, 0.25,
+                                            run, cfg["V_MAX"], ng)
+            dv = DG.compute_divb_and_write(pr, d, 0.7 * d, 1.3 * d, 0, None, comm, 0, 7, 0.25,
+                                           run, ng)
+            rec[phys + "_diag"] = np.array(res, dtype=np.float64)
+            rec[phys + "_divb"] = np.array([np.nan if x is None else x for x in dv])
+            for f in ("diagnostics.csv", "centerline.csv", "divb.csv"):
+                path = os.path.join(run, f)
+                text = open(path).read() if os.path.exists(path) else ""
+                rec[phys + "_" + f.split(".")[0] + "_csv"] = np.array(text)
+        rec[phys + "_pr"] = pr
+    np.savez_compressed(out, ng=np.array(ng), d=np.array(d), cfg=np.array(json.dumps(cfg)), **rec)
+
+
 def one(name, ref):
     out = os.path.join(HERE, name + ".npz")
     if name in CASE_BY_NAME:
@@ -308,6 +385,8 @@ def one(name, ref):
         run_source(name, ref, out)
     elif name in ("chemistry", "dissipation"):
         run_chem_dissip(name, ref, out)
+    elif name == "diagnostics":
+        run_diagnostics(name, ref, out)
     else:
         run_loop(name, ref, out)
     print("wrote", out, flush=True)
