@@ -19,9 +19,12 @@ Arms
 Timing: CUDA events on the launching stream around exactly K steps after W
 warm-up steps, barrier + synchronize on both sides, max over ranks.  Every
 array (1.6 GB each) is larger than the 126 MB L2, so no explicit flush.
-With --gpus N each rank advances its own full-size replica (the north-star path
-is single-GPU; there is no data-path collective), value = N x per-rank work /
-max time.
+With --gpus N (default --decomp slab) the ranks hold the x-slabs of one jet of
+N n x n x n cells (weak scaling: n^3 cells per GPU): once per step each rank
+swaps NG = 3 ghost layers with its x-neighbours over NCCL (send/recv, the
+reference driver's exchange), the first rank drives the nozzle and the last
+the +x outflow.  --decomp replicas runs N independent blocks instead.  value =
+N x per-rank work / max time.
 """
 import argparse
 import json
@@ -53,6 +56,9 @@ def parse():
                          "B_phi(r) jet field on the ambient Bx (the configuration as "
                          "specified); reference: the reference driver's periodic y/z, "
                          "fixed ambient inlet and By = B0 s")
+    ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
+                    help="with --gpus N > 1: x-slabs of one jet with a ghost exchange per "
+                         "step, or N independent blocks")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -92,6 +98,15 @@ def dist_init(args):
             torch.cuda.set_device(local)
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
     return rank, world, local
+
+
+def slab_domain(args, world):
+    """The x-slab of this rank in a jet of world x n cells along x, or None
+    (one GPU, or independent replicas)."""
+    if world <= 1 or args.decomp != "slab":
+        return None
+    from astrofd_b200.slabs import SlabDomain
+    return SlabDomain(args.n * world, 3)
 
 
 def barrier(world):
@@ -173,26 +188,31 @@ class ClockSampler:
 class DriverStep:
     """One reference driver-loop iteration on device tensors."""
 
-    def __init__(self, n, ng, core_cfg, nozzle_cfg, src_cfg):
+    def __init__(self, n, ng, core_cfg, nozzle_cfg, src_cfg, slab=None):
         from astrofd_b200.core import boundary, nozzle, rmhd_core, source_terms
         self.B, self.N, self.R, self.S = boundary, nozzle, rmhd_core, source_terms
         self.n, self.ng = n, ng
         self.d = 1.0 / n
         self.dt = core_cfg["CFL"] * self.d
         self.noz, self.src = nozzle_cfg, src_cfg
-        self.rng = np.random.default_rng(1234)
+        self.slab = slab
+        self.rng = np.random.default_rng(1234 + (777 * slab.rank if slab else 0))
 
     def bcs(self, pr):
         if self.noz.get("YZ_BOUNDARY") == "outflow":
             self.B.apply_outflow_yz(pr, self.ng)
         else:
             self.B.apply_periodic_yz(pr, self.ng)
-        self.B.apply_outflow_right_x(pr, self.ng)
-        self.N.apply_nozzle_left_x(pr, self.d, self.d, self.d, self.n, self.n, 0.5, 0.5,
-                                   self.rng, self.noz)
+        if self.slab is None or self.slab.last:
+            self.B.apply_outflow_right_x(pr, self.ng)
+        if self.slab is None or self.slab.first:
+            self.N.apply_nozzle_left_x(pr, self.d, self.d, self.d, self.n, self.n, 0.5, 0.5,
+                                       self.rng, self.noz)
 
     def __call__(self, pr, out, profile=False):
         d = self.d
+        if self.slab is not None:
+            self.slab.exchange(pr)
         self.bcs(pr)
         times = None
         if profile:
@@ -217,7 +237,7 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     if learned:
         from astrofd_b200 import learned_c2p
         rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
-    step = DriverStep(args.n, 3, core, noz, src)
+    step = DriverStep(args.n, 3, core, noz, src, slab_domain(args, world))
     a = torch.from_numpy(pr_host).to("cuda")
     b = torch.empty_like(a)
     for _ in range(args.warmup):
@@ -264,7 +284,7 @@ def time_e2e(args, world, prec, pr_host, cfgs, learned=False):
     if learned:
         from astrofd_b200 import learned_c2p
         rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
-    step = DriverStep(args.n, 3, core, noz, src)
+    step = DriverStep(args.n, 3, core, noz, src, slab_domain(args, world))
     host_in = torch.from_numpy(pr_host).pin_memory()
     host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
     dev_in = [torch.empty(host_in.shape, dtype=torch.float64, device="cuda") for _ in range(2)]
@@ -632,7 +652,10 @@ def main():
                    "c2p_guess": "learned" if learned else "reference",
                    "flux_mode": args.flux_mode, "boundaries": args.boundaries,
                    "l2": "inputs larger than L2 (1.6 GB arrays)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                   "parallelism": ("single GPU" if world == 1 else
+                                   f"x-slabs x{world}, 3 ghost layers exchanged per step "
+                                   "(NCCL send/recv)" if args.decomp == "slab" else
+                                   f"replicas x{world}")},
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
         "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed", learned),
