@@ -143,10 +143,8 @@ int validate(const AstroParams* p, const AstroGrid* g) {
     if (p->n_passive < 0 || p->n_passive > kMaxPassive) return ASTRO_E_UNSUPPORTED;
     if (p->n_passive > 0 && (p->passive_offset < nm || p->passive_offset + p->n_passive > g->nv))
         return ASTRO_E_SHAPE;
-    // SRHD blocks of 15+ variables carry Israel-Stewart dissipation fields whose
-    // fluxes (srhd_core.py:394-462) are outside this library's scope.
-    if (p->physics == ASTRO_SRHD && (g->nv >= 15 || (p->n_passive > 0 && p->passive_offset != 5)))
-        return ASTRO_E_UNSUPPORTED;
+    // the bulk pressure the SRHD MUSCL faces add sits in variable 5
+    if (p->physics == ASTRO_SRHD && p->passive_offset > 5 && g->nv < 6) return ASTRO_E_SHAPE;
     if (g->nx < 8 || g->ny < 8 || g->nz < 8) return ASTRO_E_SHAPE;
     // cell indices are 32-bit in the kernels; 2^31 cells of even 5 float64
     // variables exceed the device memory
@@ -167,6 +165,7 @@ struct FaceArgs {
     void* aux;           // R[4][nc]: sL, sR, vL, vR (or null)
     void* speeds_out;    // R[2][nc]: sL, sR (z faces, carried mode) or null
     const void* carried; // R[2][nc]: z-face speeds read by the carried x faces
+    int ndiss;           // SRHD Israel-Stewart blocks: dissipation fluxes per face
     AstroParams p;
     // float32 passes: faces whose float32 result is not finite are listed here
     // and recomputed in float64 by k_face_fix
@@ -223,7 +222,23 @@ __device__ __forceinline__ bool face_at(const FaceArgs& a, int i, int j, int k) 
         }
     }
     if (PHYS == ASTRO_SRHD) {
-        s_face<RIEMANN>(P, DIR, qL, qR, F, sL, sR);
+        if (RECON == ASTRO_RECON_MUSCL && a.p.passive_offset > 5) {
+            // add_pi_lr (srhd_core.py:394-398): the cells' bulk pressure on
+            // the reconstructed face pressures, before the floor
+            qL[4] += (R)__ldg(a.pr + 5 * nc + cell - stride);
+            qR[4] += (R)__ldg(a.pr + 5 * nc + cell);
+        }
+        if (a.ndiss > 0) {
+            R isL[10], isR[10];
+#pragma unroll
+            for (int m = 0; m < 10; ++m) {
+                isL[m] = (R)__ldg(a.pr + (size_t)(5 + m) * nc + cell - stride);
+                isR[m] = (R)__ldg(a.pr + (size_t)(5 + m) * nc + cell);
+            }
+            s_face<RIEMANN>(P, DIR, qL, qR, F, sL, sR, a.ndiss, isL, isR);
+        } else {
+            s_face<RIEMANN>(P, DIR, qL, qR, F, sL, sR);
+        }
     } else {
         r_face<RIEMANN, RECON == ASTRO_RECON_MUSCL, GIVEN>(P, DIR, qL, qR, F, sL, sR);
     }
@@ -503,7 +518,11 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 6) k_update(UpdArg
             for (int v = NM; v < a.nv; ++v) {
                 double out = 0.0;
                 const int t = v - po;
-                if (np > 0 && t >= 0 && t < np) {
+                if (PHYS == ASTRO_SRHD && v < po) {
+                    // Israel-Stewart fields 5..PASSIVE_OFFSET-1: carried from
+                    // the stage input (srhd_core.py:1309-1310)
+                    out = a.prk[(size_t)v * nc + cell];
+                } else if (np > 0 && t >= 0 && t < np) {
                     const size_t o = (size_t)v * nc + cell;
                     const double t0 = a.pr0[o], r = rp[t];
                     if (a.stage == 0) out = __dadd_rn(t0, __dmul_rn(dt, r));
@@ -853,6 +872,17 @@ cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
 
 // All face passes of one stage: z (with speeds in carried mode), x, carried x, y.
 // prf_ready: the float32 copy of pr was written by the kernel that produced pr
+// SRHD blocks of 15+ variables carry Israel-Stewart fields whose fluxes the
+// reference adds to every MUSCL face once and to every PPM face twice
+// (srhd_core.py:543-544, 958-961) and not in WENO; conservative mode adds
+// them once for PPM too.
+int dissipation_fluxes(const AstroParams& p, const AstroGrid& g) {
+    if (p.physics != ASTRO_SRHD || g.nv < 15) return 0;
+    if (p.recon == ASTRO_RECON_MUSCL) return 1;
+    if (p.recon == ASTRO_RECON_PPM) return p.flux_mode == ASTRO_FLUX_CONSERVATIVE ? 1 : 2;
+    return 0;
+}
+
 cudaError_t face_passes(const AstroParams& p, const AstroGrid& g, const Bounds& b,
                         const double* pr, char* work, const Layout& L, cudaStream_t s,
                         bool prf_ready = false) {
@@ -870,6 +900,7 @@ cudaError_t face_passes(const AstroParams& p, const AstroGrid& g, const Bounds& 
         FaceArgs a;
         memset(&a, 0, sizeof(a));
         a.pr = pr; a.prf = prf; a.nx = g.nx; a.ny = g.ny; a.nz = g.nz; a.dir = d; a.b = b; a.p = p;
+        a.ndiss = dissipation_fluxes(p, g);
         for (int e = 0; e < 3; ++e) {
             a.org[e] = b.lo;
             a.ext[e] = b.hi[e] - b.lo + (e == d ? 1 : 0);

@@ -340,9 +340,26 @@ AHD void hllc5(int n, const R* UL, const R* UR, const R* FL, const R* FR, R sL, 
     for (int v = 0; v < 5; ++v) out[v] = F[v] + s * (Ust[v] - U[v]);
 }
 
-// one SRHD face: floor, p2c, flux, speeds, Riemann (srhd_core.py:517-532)
+// Israel-Stewart dissipation flux of one cell added to a face flux
+// (add_diss_flux_x/y/z, srhd_core.py:417-442).  is = pi, pixx, piyy, pizz,
+// pixy, pixz, piyz, qx, qy, qz of the cell; q the face primitives after the
+// floor.  Stress row n: pi delta_nm + pi^nm; energy: v . row + q_n, summed in
+// the reference's order.
+template <typename R> AHD void s_diss_flux(int n, const R* q, const R* is, R* F) {
+    constexpr int S[3][3] = {{1, 4, 5}, {4, 2, 6}, {5, 6, 3}};
+    R row[3];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) row[m] = (m == n) ? is[0] + is[S[n][m]] : is[S[n][m]];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) F[1 + m] += row[m];
+    F[4] += q[1] * row[0] + q[2] * row[1] + q[3] * row[2] + is[7 + n];
+}
+
+// one SRHD face: floor, p2c, flux, (ndiss times the dissipation fluxes of the
+// cells isL / isR), speeds, Riemann (srhd_core.py:517-550)
 template <int RIEMANN, typename R>
-AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
+AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR, int ndiss = 0,
+                const R* isL = nullptr, const R* isR = nullptr) {
     R UL[5], UR[5], FL[5], FR[5], lmL, lpL, lmR, lpR;
     floor_prim(P, qL);
     floor_prim(P, qR);
@@ -350,6 +367,10 @@ AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
     s_p2c(P, qR, UR);
     s_flux_u(P, n, qL, UL, FL);
     s_flux_u(P, n, qR, UR, FR);
+    for (int rep = 0; rep < ndiss; ++rep) {
+        s_diss_flux(n, qL, isL, FL);
+        s_diss_flux(n, qR, isR, FR);
+    }
     R csL = s_sound_speed(P, qL[0], qL[4]), csR = s_sound_speed(P, qR[0], qR[4]);
     eig_speeds(qL[1 + n], csL, lmL, lpL);
     eig_speeds(qR[1 + n], csR, lmR, lpR);

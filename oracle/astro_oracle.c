@@ -308,9 +308,23 @@ static double contact_speed(int n, const double* UL, const double* UR, double sL
 
 typedef struct { double F[9]; double sL, sR, vL, vR; } Face;
 
+/* Israel-Stewart dissipation flux of one cell added to a face flux
+ * (add_diss_flux_x/y/z, srhd_core.py:417-442): is = pi, pixx, piyy, pizz,
+ * pixy, pixz, piyz, qx, qy, qz of the cell, q the face primitives after the
+ * floor.  Row n of the stress: pi delta_nm + pi^nm; energy: v.row + q_n. */
+static void s_diss_flux(int n, const double* q, const double* is, double* F) {
+    static const int S[3][3] = {{1, 4, 5}, {4, 2, 6}, {5, 6, 3}};
+    double row[3];
+    for (int m = 0; m < 3; ++m) row[m] = (m == n) ? is[0] + is[S[n][m]] : is[S[n][m]];
+    for (int m = 0; m < 3; ++m) F[1 + m] += row[m];
+    F[4] += q[1] * row[0] + q[2] * row[1] + q[3] * row[2] + is[7 + n];
+}
+
 /* One SRHD face from reconstructed left/right primitives: floor, p2c, flux,
- * speeds, Riemann (the repeated block of srhd_core.py:517-532 etc.). */
-static void s_face(const OParams* pa, int n, double* qL, double* qR, Face* f) {
+ * (ndiss times the dissipation fluxes of the cells isL / isR), speeds,
+ * Riemann (the repeated block of srhd_core.py:517-550 etc.). */
+static void s_face_is(const OParams* pa, int n, double* qL, double* qR, int ndiss,
+                      const double* isL, const double* isR, Face* f) {
     double UL[5], UR[5], FL[5], FR[5], lmL, lpL, lmR, lpR;
     s_floor(pa, qL);
     s_floor(pa, qR);
@@ -318,6 +332,10 @@ static void s_face(const OParams* pa, int n, double* qL, double* qR, Face* f) {
     s_p2c(qR, UR);
     s_flux(n, qL, FL);
     s_flux(n, qR, FR);
+    for (int rep = 0; rep < ndiss; ++rep) {
+        s_diss_flux(n, qL, isL, FL);
+        s_diss_flux(n, qR, isR, FR);
+    }
     double csL = s_sound_speed(qL[0], qL[4]), csR = s_sound_speed(qR[0], qR[4]);
     eig_speeds(qL[1 + n], csL, &lmL, &lpL);
     eig_speeds(qR[1 + n], csR, &lmR, &lpR);
@@ -327,6 +345,10 @@ static void s_face(const OParams* pa, int n, double* qL, double* qR, Face* f) {
     else
         hlle_vec(5, UL, UR, FL, FR, sL, sR, f->F);
     f->sL = sL; f->sR = sR; f->vL = qL[1 + n]; f->vR = qR[1 + n];
+}
+
+static void s_face(const OParams* pa, int n, double* qL, double* qR, Face* f) {
+    s_face_is(pa, n, qL, qR, 0, NULL, NULL, f);
 }
 
 /* ------------------------------------------------------------------ */
@@ -848,8 +870,19 @@ static void s_rhs(const OParams* pa, const OGrid* g, const double* pr, double dd
                         qL2[4] += P(5, i, j, k);
                         qR2[4] += P(5, o[0], o[1], o[2]);
                     }
-                    s_face(pa, n, qL, qR, &fa);
-                    s_face(pa, n, qL2, qR2, &fb);
+                    /* dissipation fluxes of blocks of 15+ variables: once in
+                     * MUSCL, twice in PPM (srhd_core.py:543-544, 958-961),
+                     * none in WENO */
+                    const int nd = g->nv >= 15 ? (pa->recon == 0 ? 1 : (pa->recon == 1 ? 2 : 0)) : 0;
+                    double isA[10], isB[10], isC[10];
+                    if (nd)
+                        for (int m = 0; m < 10; ++m) {
+                            isA[m] = P(5 + m, i - DI[n][0], j - DI[n][1], k - DI[n][2]);
+                            isB[m] = P(5 + m, i, j, k);
+                            isC[m] = P(5 + m, o[0], o[1], o[2]);
+                        }
+                    s_face_is(pa, n, qL, qR, nd, isA, isB, &fa);
+                    s_face_is(pa, n, qL2, qR2, nd, isB, isC, &fb);
                     for (int v = 0; v < 5; ++v) r[v] -= (fb.F[v] - fa.F[v]) / dd[n];
                     /* passives */
                     int kinds[3], nk = 0, lkind = -1;
@@ -961,7 +994,6 @@ int oracle_rhs(const OParams* pa, const double* pr, int nv, int nx, int ny, int 
     OGrid g = {nv, nx, ny, nz};
     double dd[3] = {dx, dy, dz};
     if (pa->physics == 0) {
-        if (nv >= 15) return -2; /* Israel-Stewart dissipation fluxes: out of scope */
         s_rhs(pa, &g, pr, dd, rhs);
     } else {
         r_rhs(pa, &g, pr, dd, rhs);
@@ -1021,7 +1053,6 @@ int oracle_step(const OParams* pa, const double* pr, int nv, int nx, int ny, int
     const int np = pa->n_passive, po = pa->passive_offset;
     const size_t nc = (size_t)nx * ny * nz;
     const int nr = nm + np;
-    if (pa->physics == 0 && nv >= 15) return -2;
     double* U0 = malloc(sizeof(double) * nm * nc);
     double* Uk = malloc(sizeof(double) * nm * nc);
     double* rhs = malloc(sizeof(double) * nr * nc);

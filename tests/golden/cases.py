@@ -50,6 +50,17 @@ CASES = [
     # configured Gamma=4/3 is ignored by the SRHD kernels (frozen default arg)
     _c("s_muscl_mc_hlle_gamma43", "srhd", "muscl", "mc", "hlle", 2, 2, seed=111,
        GAMMA=4.0 / 3.0),
+    # Israel-Stewart blocks (15+ variables, passives from 15): bulk pressure
+    # added to the MUSCL face pressures, dissipation fluxes once (MUSCL),
+    # twice (PPM) or not at all (WENO), fields 5..14 carried by the step
+    _c("s_muscl_mc_hlle_is", "srhd", "muscl", "mc", "hlle", 2, 2, seed=112,
+       state=dict(n_is=10), PASSIVE_OFFSET=15),
+    _c("s_muscl_minmod_hllc_is_pass1", "srhd", "muscl", "minmod", "hllc", 3, 3, n_extra=1,
+       pad=1, seed=113, state=dict(n_is=10), PASSIVE_OFFSET=15),
+    _c("s_ppm_hllc_is", "srhd", "ppm", "mc", "hllc", 3, 3, seed=114, state=dict(n_is=10),
+       PASSIVE_OFFSET=15),
+    _c("s_weno_hlle_is", "srhd", "weno", "mc", "hlle", 2, 3, seed=115, state=dict(n_is=10),
+       PASSIVE_OFFSET=15),
     # ---- RMHD --------------------------------------------------------
     _c("r_muscl_mc_hlle_rk2", "rmhd", "muscl", "mc", "hlle", 2, 2, seed=201),
     _c("r_muscl_minmod_hlld_rk2", "rmhd", "muscl", "minmod", "hlld", 2, 2, seed=202),

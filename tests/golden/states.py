@@ -17,7 +17,7 @@ def n_main(physics):
 
 
 def make_state(seed, n, ng, physics, n_extra=0, vjet=0.99, noise=0.3,
-               bamp=0.3, stripes=True):
+               bamp=0.3, stripes=True, n_is=0):
     """Return a rough jet-like primitive block.
 
     n        interior cells per dimension (cube)
@@ -25,11 +25,13 @@ def make_state(seed, n, ng, physics, n_extra=0, vjet=0.99, noise=0.3,
     physics  "srhd" (5 primitives) or "rmhd" (9 primitives)
     n_extra  extra passive variables appended after the base primitives
     stripes  leave every third x-plane ambient (strong shocks) when True
+    n_is     Israel-Stewart fields (pi, pi^ij, q^i: 10) between the base
+             primitives and the passives (SRHD blocks of 15+ variables)
     """
     rng = np.random.default_rng(seed)
     N = n + 2 * ng
     nm = n_main(physics)
-    nv = nm + n_extra
+    nv = nm + n_is + n_extra
     pr = np.zeros((nv, N, N, N), dtype=np.float64)
 
     def u(*shape):
@@ -65,8 +67,10 @@ def make_state(seed, n, ng, physics, n_extra=0, vjet=0.99, noise=0.3,
         pr[7] = bamp * u(N, N, N)
         pr[8] = 0.01 * u(N, N, N)
 
+    for m in range(n_is):
+        pr[nm + m] = 0.003 * u(N, N, N)
     for t in range(n_extra):
-        pr[nm + t] = rng.random((N, N, N))
+        pr[nm + n_is + t] = rng.random((N, N, N))
     return np.ascontiguousarray(pr)
 
 

@@ -56,9 +56,13 @@ def test_error_strings_and_validation(lib):
     p.riemann = 7
     assert lib.astro_step_workspace_bytes(C.byref(p), C.byref(g)) == 0
     assert lib.astro_rhs(C.byref(p), C.byref(g), None, None, None, 0, None) == -1
-    # SRHD blocks carrying dissipation fields are rejected
+    # SRHD blocks carrying Israel-Stewart fields (15 variables, passives from
+    # 15) are accepted; a bulk-pressure offset past a 5-variable block is not
     p.physics, p.riemann = 0, 0
+    p.passive_offset = 15
     g.nv = 15
+    assert lib.astro_rhs_workspace_bytes(C.byref(p), C.byref(g)) > 0
+    g.nv = 5
     assert lib.astro_rhs_workspace_bytes(C.byref(p), C.byref(g)) == 0
 
 
