@@ -69,6 +69,14 @@ class AstroDissipation(C.Structure):
                 ("p_max", C.c_double)]
 
 
+class AstroGR(C.Structure):
+    _fields_ = [("metric", C.c_int32), ("orthonormal_flux", C.c_int32), ("ng", C.c_int32),
+                ("offs_x", C.c_int32), ("mass", C.c_double), ("spin", C.c_double)]
+
+
+GR_MINKOWSKI, GR_SCHWARZSCHILD, GR_KERR_SCHILD, GR_OTHER = 0, 1, 2, 3
+
+
 class AstroC2PStats(C.Structure):
     _fields_ = [(n, C.c_ulonglong) for n in
                 ("cells", "newton", "bisection", "hydro_fallback", "learned_polish",
@@ -107,6 +115,12 @@ PROTOS = {
                                       C.c_double, _VP]),
     "astro_diagnostics": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), C.c_int, _DP,
                                     C.c_double, _DP, _VP]),
+    "astro_gr_workspace_bytes": (C.c_size_t, [C.POINTER(AstroParams), C.POINTER(AstroGrid),
+                                              C.POINTER(AstroGR), C.c_int]),
+    "astro_rhs_gr": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), C.POINTER(AstroGR),
+                               _DP, _DP, _VP, C.c_size_t, _VP]),
+    "astro_step_gr": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), C.POINTER(AstroGR),
+                                _DP, _DP, C.c_double, C.c_int, _VP, C.c_size_t, _VP, _VP]),
     "astro_causal_dissipation_workspace_bytes": (C.c_size_t, [C.POINTER(AstroGrid)]),
     "astro_causal_dissipation": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroDissipation),
                                            C.c_double, _VP, C.c_size_t, _VP]),

@@ -125,6 +125,40 @@ class Engine:
                                 rt.stream_handle(t.device)), "astro_step")
         return out.cpu().numpy() if was_np else out
 
+    # -- fixed-metric GR wrappers -------------------------------------------
+    def rhs_gr(self, gr, pr, dx, dy, dz):
+        L = _lib.load()
+        t, was_np = rt.to_device(pr)
+        grid = rt.grid_of(t, dx, dy, dz)
+        nx, ny, nz = t.shape[1:]
+        out = torch.empty((self.nm + self.p.n_passive, nx, ny, nz), dtype=torch.float64,
+                          device=t.device)
+        nb = L.astro_gr_workspace_bytes(C.byref(self.p), C.byref(grid), C.byref(gr), 0)
+        if nb == 0:
+            _lib.check(-4, "astro_rhs_gr (configuration)")
+        w = rt.workspace(nb, t.device)
+        _lib.check(L.astro_rhs_gr(C.byref(self.p), C.byref(grid), C.byref(gr), rt.ptr(t),
+                                  rt.ptr(out), rt.ptr(w), nb, rt.stream_handle(t.device)),
+                   "astro_rhs_gr")
+        return out.cpu().numpy() if was_np else out
+
+    def step_gr(self, gr, pr, dx, dy, dz, dt, rk_order, out=None):
+        L = _lib.load()
+        t, was_np = rt.to_device(pr)
+        grid = rt.grid_of(t, dx, dy, dz)
+        if out is None:
+            out = torch.empty_like(t)
+        nb = L.astro_gr_workspace_bytes(C.byref(self.p), C.byref(grid), C.byref(gr), 1)
+        if nb == 0:
+            _lib.check(-4, "astro_step_gr (configuration)")
+        self._require_network()
+        w = rt.workspace(nb, t.device)
+        stats = self._stats_buffer(t.device)
+        _lib.check(L.astro_step_gr(C.byref(self.p), C.byref(grid), C.byref(gr), rt.ptr(t),
+                                   rt.ptr(out), float(dt), int(rk_order), rt.ptr(w), nb,
+                                   rt.ptr(stats), rt.stream_handle(t.device)), "astro_step_gr")
+        return out.cpu().numpy() if was_np else out
+
     def step_profiled(self, pr, dx, dy, dz, dt, rk_order, out):
         """One step with per-kernel-class CUDA-event times (synchronises)."""
         L = _lib.load()

@@ -862,8 +862,10 @@ cudaError_t launch_update(const UpdArgs& a, cudaStream_t s) {
             else launch_update_t<PH, double, DEF, false>(a, grd, blk, s);          \
         }                                                                          \
     } while (0)
-    if (a.p.physics == ASTRO_SRHD) UPD(ASTRO_SRHD, false);
-    else if (a.defer_c2p) UPD(ASTRO_RMHD, true);
+    if (a.p.physics == ASTRO_SRHD) {
+        if (a.defer_c2p) UPD(ASTRO_SRHD, true);  // GR steps: con2prim after the sources
+        else UPD(ASTRO_SRHD, false);
+    } else if (a.defer_c2p) UPD(ASTRO_RMHD, true);
     else UPD(ASTRO_RMHD, false);
 #undef UPD
     mark(1, s);
@@ -1402,6 +1404,107 @@ __global__ void k_diagnostics(AstroParams p, const double* pr, int nv, int nx, i
     }
 }
 
+// ------------------------------------------------- fixed-metric GR ---
+// lapse helpers of gr_metric.py:6-38 (r offset by 1e-12 as there)
+__device__ __forceinline__ double gr_radius(double x, double y, double z) {
+    return sqrt(x * x + y * y + z * z) + 1e-12;
+}
+
+__device__ __forceinline__ double gr_ks_alpha(double x, double y, double z, double M) {
+    const double H = M / gr_radius(x, y, z);
+    return 1.0 / sqrt(1.0 + 2.0 * H);
+}
+
+// grad ln(alpha): isotropic Schwarzschild lapse, or Kerr-Schild (spin 0)
+__device__ __forceinline__ void gr_dlna(int metric, double x, double y, double z, double M,
+                                        double* g) {
+    const double r = gr_radius(x, y, z);
+    double dlnadr;
+    if (metric == ASTRO_GR_SCHWARZSCHILD) {
+        const double a = M / (2.0 * r);
+        const double denom = 1.0 - a * a;
+        dlnadr = denom == 0.0 ? 0.0 : (2.0 * a) / (r * denom);
+    } else {
+        const double H = M / r;
+        dlnadr = H / (r * (1.0 + 2.0 * H));
+    }
+    g[0] = dlnadr * (x / r);
+    g[1] = dlnadr * (y / r);
+    g[2] = dlnadr * (z / r);
+}
+
+struct GRGeom {
+    int nx, ny, nz, ng, offs_x;
+    double dx, dy, dz, mass;
+    __device__ bool interior(unsigned c, int& i, int& j, int& k, double& x, double& y,
+                             double& z) const {
+        k = (int)(c % (unsigned)nz);
+        const unsigned r = c / (unsigned)nz;
+        j = (int)(r % (unsigned)ny);
+        i = (int)(r / (unsigned)ny);
+        if (i < ng || i >= nx - ng || j < ng || j >= ny - ng || k < ng || k >= nz - ng)
+            return false;
+        x = (offs_x + (i - ng) + 0.5) * dx;
+        y = (j - ng + 0.5) * dy;
+        z = (k - ng + 0.5) * dz;
+        return true;
+    }
+};
+
+// copy of the block with the interior velocities divided by max(alpha_KS,
+// 1e-12): what the flux passes see (grhd_core.py:22-37)
+__global__ void k_gr_rescale(const double* __restrict__ pr, double* __restrict__ out, int nv,
+                             GRGeom G) {
+    const unsigned nc = (unsigned)G.nx * G.ny * G.nz;
+    for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        int i, j, k;
+        double x, y, z;
+        const bool in = G.interior(c, i, j, k, x, y, z);
+        const double ax = in ? rmax(gr_ks_alpha(x, y, z, G.mass), 1e-12) : 1.0;
+        for (int v = 0; v < nv; ++v) {
+            const double q = pr[(size_t)v * nc + c];
+            out[(size_t)v * nc + c] = (in && v >= 1 && v <= 3) ? q / ax : q;
+        }
+    }
+}
+
+// out[1..4] += coef * source over the interior (grhd_core.py:47-78,
+// grmhd_core.py:47-80); out is a right-hand side (coef 1) or the stage's
+// conserved state (coef = the stage's weight of dt * rhs)
+__global__ void k_gr_source(AstroParams p, int metric, const double* __restrict__ pr,
+                            double* __restrict__ out, GRGeom G, double coef) {
+    const unsigned nc = (unsigned)G.nx * G.ny * G.nz;
+    const bool mhd = p.physics == ASTRO_RMHD;
+    const Phys<double> P = Phys<double>::from(p);
+    const double gfac = p.gamma / (p.gamma - 1.0);
+    for (unsigned c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+        int i, j, k;
+        double x, y, z;
+        if (!G.interior(c, i, j, k, x, y, z)) continue;
+        double g[3];
+        gr_dlna(metric, x, y, z, G.mass, g);
+        double q[9], U[9];
+        for (int v = 0; v < (mhd ? 9 : 5); ++v) q[v] = pr[(size_t)v * nc + c];
+        double v2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+        if (v2 >= 1.0) v2 = 1.0 - 1e-14;
+        const double W = 1.0 / sqrt(1.0 - v2);
+        const double h = 1.0 + gfac * q[4] / rmax(q[0], 1e-12);
+        double w = q[0] * h * W * W;
+        if (mhd) {
+            w = w + (q[5] * q[5] + q[6] * q[6] + q[7] * q[7]);
+            r_p2c(P, q, U);
+        } else {
+            s_p2c(P, q, U);
+        }
+        w = w + q[4];
+        double* o = out + c;
+        o[(size_t)1 * nc] += coef * (w * g[0]);
+        o[(size_t)2 * nc] += coef * (w * g[1]);
+        o[(size_t)3 * nc] += coef * (w * g[2]);
+        o[(size_t)4 * nc] += coef * (U[1] * g[0] + U[2] * g[1] + U[3] * g[2]);
+    }
+}
+
 int grid_for(size_t n, int block) {
     size_t g = (n + block - 1) / block;
     if (g > 148 * 32) g = 148 * 32;
@@ -1717,6 +1820,132 @@ int astro_causal_dissipation(double* pr, const AstroGrid* g, const AstroDissipat
                                                     g->dy, g->dz);
     mark(2, s);
     return cuda_status(cudaGetLastError());
+}
+
+static int gr_check(const AstroParams* p, const AstroGrid* g, const AstroGR* gr) {
+    int v = validate(p, g);
+    if (v != ASTRO_OK) return v;
+    if (!gr || gr->metric < ASTRO_GR_MINKOWSKI || gr->metric > ASTRO_GR_OTHER) return ASTRO_E_INVALID;
+    if (gr->ng < 0 || 2 * gr->ng >= g->nx || 2 * gr->ng >= g->ny || 2 * gr->ng >= g->nz)
+        return ASTRO_E_SHAPE;
+    if (!(gr->mass == gr->mass)) return ASTRO_E_INVALID;
+    return ASTRO_OK;
+}
+
+static bool gr_rescales(const AstroGR& gr) {
+    return gr.orthonormal_flux &&
+           (gr.metric == ASTRO_GR_SCHWARZSCHILD || gr.metric == ASTRO_GR_KERR_SCHILD);
+}
+
+static GRGeom gr_geom(const AstroGrid& g, const AstroGR& gr) {
+    GRGeom G;
+    G.nx = g.nx; G.ny = g.ny; G.nz = g.nz; G.ng = gr.ng; G.offs_x = gr.offs_x;
+    G.dx = g.dx; G.dy = g.dy; G.dz = g.dz; G.mass = gr.mass;
+    return G;
+}
+
+size_t astro_gr_workspace_bytes(const AstroParams* p, const AstroGrid* g, const AstroGR* gr,
+                                int step) {
+    if (gr_check(p, g, gr) != ASTRO_OK) return 0;
+    const size_t nc = (size_t)g->nx * g->ny * g->nz;
+    return layout_of(*p, *g, step != 0).total +
+           (gr_rescales(*gr) ? align256((size_t)g->nv * nc * 8) : 0);
+}
+
+// the flux passes' input: pr, or its rescaled copy at the end of the workspace
+static const double* gr_flux_input(const AstroGR& gr, const AstroGrid& g, const double* pr,
+                                   char* w, size_t off, cudaStream_t s) {
+    if (!gr_rescales(gr)) return pr;
+    double* out = (double*)(w + off);
+    const size_t nc = (size_t)g.nx * g.ny * g.nz;
+    k_gr_rescale<<<grid_for(nc, 256), 256, 0, s>>>(pr, out, g.nv, gr_geom(g, gr));
+    mark(2, s);
+    return out;
+}
+
+int astro_rhs_gr(const AstroParams* p, const AstroGrid* g, const AstroGR* gr, const double* pr,
+                 double* rhs, void* work, size_t work_bytes, void* stream) {
+    int v = gr_check(p, g, gr);
+    if (v != ASTRO_OK) return v;
+    if (!pr || !rhs) return ASTRO_E_INVALID;
+    const Layout L = layout_of(*p, *g, false);
+    if (!work || work_bytes < astro_gr_workspace_bytes(p, g, gr, 0)) return ASTRO_E_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* w = (char*)work;
+    const Bounds b = bounds_of(*p, *g);
+    const double* fin = gr_flux_input(*gr, *g, pr, w, L.total, s);
+    cudaError_t e = face_passes(*p, *g, b, fin, w, L, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    UpdArgs u = update_args(*p, *g, b, w, L);
+    u.pr0 = pr; u.prk = pr; u.dst = rhs; u.rhs_only = 1;
+    e = launch_update(u, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    if (gr->metric != ASTRO_GR_MINKOWSKI) {
+        const size_t nc = (size_t)g->nx * g->ny * g->nz;
+        k_gr_source<<<grid_for(nc, 256), 256, 0, s>>>(*p, gr->metric, pr, rhs, gr_geom(*g, *gr),
+                                                      1.0);
+        mark(2, s);
+    }
+    return cuda_status(cudaGetLastError());
+}
+
+int astro_step_gr(const AstroParams* p, const AstroGrid* g, const AstroGR* gr,
+                  const double* pr_in, double* pr_out, double dt, int rk_order, void* work,
+                  size_t work_bytes, AstroC2PStats* stats, void* stream) {
+    int v = gr_check(p, g, gr);
+    if (v != ASTRO_OK) return v;
+    if (!pr_in || !pr_out || pr_in == pr_out) return ASTRO_E_INVALID;
+    if (rk_order != 2 && rk_order != 3) return ASTRO_E_INVALID;
+    const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
+    if (p->c2p_guess != ASTRO_GUESS_REFERENCE && !learned) return ASTRO_E_INVALID;
+    if (learned && (p->physics != ASTRO_RMHD || !p->mlp)) return ASTRO_E_UNSUPPORTED;
+    const Layout L = layout_of(*p, *g, true);
+    if (!work || work_bytes < astro_gr_workspace_bytes(p, g, gr, 1)) return ASTRO_E_WORKSPACE;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* w = (char*)work;
+    const Bounds b = bounds_of(*p, *g);
+    const int nst = rk_order;
+    const size_t nc = (size_t)g->nx * g->ny * g->nz;
+    const double* cur = pr_in;
+    double* bufs[2] = {(double*)(w + L.prA), (double*)(w + L.prB)};
+    double* U = (double*)(w + L.U);
+    for (int st = 0; st < nst; ++st) {
+        // the update writes U only; the sources are added to U with the
+        // stage's weight of dt * rhs, then con2prim gives the primitives
+        const double* fin = gr_flux_input(*gr, *g, cur, w, L.total, s);
+        cudaError_t e = face_passes(*p, *g, b, fin, w, L, s);
+        if (e != cudaSuccess) return ASTRO_E_CUDA;
+        double* dst = (st == nst - 1) ? pr_out : bufs[st % 2];
+        UpdArgs u = update_args(*p, *g, b, w, L);
+        u.pr0 = pr_in; u.prk = cur; u.U = U; u.dst = dst; u.dstf = nullptr;
+        u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
+        u.defer_c2p = 1;
+        e = launch_update(u, s);
+        if (e != cudaSuccess) return ASTRO_E_CUDA;
+        if (gr->metric != ASTRO_GR_MINKOWSKI) {
+            const double wgt = st == 0 ? 1.0 : (nst == 2 ? 0.5 : (st == 1 ? 0.25 : 2.0 / 3.0));
+            k_gr_source<<<grid_for(nc, 256), 256, 0, s>>>(*p, gr->metric, cur, U,
+                                                          gr_geom(*g, *gr), wgt * dt);
+            mark(2, s);
+        }
+        if (learned) {
+            C2PArgs c;
+            c.U = U; c.q = dst; c.count = (long)nc;
+            c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
+            c.status = nullptr; c.max_polish = 2;
+            c.fb_count = (unsigned*)(w + L.c2pfb);
+            c.fb_list = (unsigned*)(w + L.c2pfb + 256);
+            c.fb_cap = (unsigned)c2p_fb_capacity(*g);
+            e = launch_c2p_learned(c, s);
+        } else {
+            k_c2p<<<sm_count_cached() * 8, 128, 0, s>>>(*p, U, dst, (long)nc, stats);
+            mark(2, s);
+            e = cudaGetLastError();
+        }
+        if (e != cudaSuccess) return ASTRO_E_CUDA;
+        cur = dst;
+    }
+    return ASTRO_OK;
 }
 
 int astro_diagnostics(const AstroParams* p, const AstroGrid* g, int ng, const double* pr,

@@ -298,6 +298,43 @@ int astro_diagnostics(const AstroParams* p, const AstroGrid* g, int ng, const do
 int astro_causal_dissipation(double* pr, const AstroGrid* g, const AstroDissipation* c, double dt,
                              void* work, size_t work_bytes, void* stream);
 
+/* --- fixed-metric GR wrappers (core/grhd_core.py, core/grmhd_core.py) -----
+ * The SRHD / RMHD right-hand side of p (physics selects GRHD or GRMHD) with
+ * the reference's approximate fixed-metric terms (metrics of
+ * core/gr_metric.py:6-38, black hole of mass `mass` at the origin, cell
+ * centres x = (offs_x + i - ng + 1/2) dx, y = (j - ng + 1/2) dy, ...):
+ *  - SCHWARZSCHILD / KERR_SCHILD with orthonormal_flux: the fluxes see the
+ *    interior velocities divided by the Kerr-Schild lapse (both metrics, as
+ *    the reference; grhd_core.py:22-37);
+ *  - every metric but MINKOWSKI: interior sources rhs[S_i] += w dln(alpha)/dx_i,
+ *    rhs[tau] += S . grad ln(alpha), w = rho h W^2 + p (+ B^2 for GRMHD), h from
+ *    the configured gamma, S from prim_to_cons (grhd_core.py:47-78); the
+ *    isotropic Schwarzschild lapse for SCHWARZSCHILD, Kerr-Schild otherwise
+ *    (OTHER: any other metric name, which the reference sends down the
+ *    Kerr-Schild branch without the rescale).  spin is unused, as there. */
+#define ASTRO_GR_MINKOWSKI 0
+#define ASTRO_GR_SCHWARZSCHILD 1
+#define ASTRO_GR_KERR_SCHILD 2
+#define ASTRO_GR_OTHER 3
+typedef struct AstroGR {
+    int32_t metric, orthonormal_flux;  /* GR_METRIC, ORTHONORMAL_FLUX          */
+    int32_t ng, offs_x;                /* ghost layers, first interior x index */
+    double mass, spin;                 /* GR_MASS, GR_SPIN                     */
+} AstroGR;
+/* workspace of astro_rhs_gr (step = 0) or astro_step_gr (step = 1); 0 on a
+ * bad configuration */
+size_t astro_gr_workspace_bytes(const AstroParams* p, const AstroGrid* g, const AstroGR* gr,
+                                int step);
+/* compute_rhs_grhd (grhd_core.py:20) / compute_rhs_grmhd (grmhd_core.py:20) */
+int astro_rhs_gr(const AstroParams* p, const AstroGrid* g, const AstroGR* gr, const double* pr,
+                 double* rhs, void* work, size_t work_bytes, void* stream);
+/* step_ssprk2/3 (grhd_core.py:76,124; grmhd_core.py:80,...): the core step
+ * with the GR right-hand side; the learned con2prim guess works as in
+ * astro_step */
+int astro_step_gr(const AstroParams* p, const AstroGrid* g, const AstroGR* gr,
+                  const double* pr_in, double* pr_out, double dt, int rk_order, void* work,
+                  size_t work_bytes, AstroC2PStats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

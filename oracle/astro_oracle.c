@@ -1046,9 +1046,111 @@ double oracle_max_char_speed(const double* pr, int nv, int nx, int ny, int nz) {
     return amax;
 }
 
+/* ------------------------------------------------------------------ */
+/* fixed-metric GR wrappers (grhd_core.py, grmhd_core.py, gr_metric.py) */
+/* ------------------------------------------------------------------ */
+typedef struct { int metric, orthonormal, ng, offs_x; double mass, spin; } OGR;
+enum { GR_MINK = 0, GR_SCHW = 1, GR_KS = 2, GR_OTHER = 3 };
+
+/* gr_metric.py:19-36 (lapse of the Kerr-Schild form; shift unused) */
+static void gr_ks(double x, double y, double z, double M, double* alpha, double g[3]) {
+    double r = sqrt(x * x + y * y + z * z) + 1e-12;
+    double H = M / r;
+    *alpha = 1.0 / sqrt(1.0 + 2.0 * H);
+    double lx = x / r, ly = y / r, lz = z / r;
+    double dlnadr = H / (r * (1.0 + 2.0 * H));
+    g[0] = dlnadr * lx; g[1] = dlnadr * ly; g[2] = dlnadr * lz;
+}
+
+/* gr_metric.py:6-16 */
+static void gr_iso(double x, double y, double z, double M, double g[3]) {
+    double r = sqrt(x * x + y * y + z * z) + 1e-12;
+    double a = M / (2.0 * r);
+    double denom = (1.0 - a * a);
+    double dlnadr = denom == 0.0 ? 0.0 : (2.0 * a) / (r * denom);
+    g[0] = dlnadr * (x / r); g[1] = dlnadr * (y / r); g[2] = dlnadr * (z / r);
+}
+
+/* compute_rhs_grhd / compute_rhs_grmhd (grhd_core.py:20-78,
+ * grmhd_core.py:20-80): velocity rescale for the fluxes, core RHS, sources */
+int oracle_rhs_gr(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
+                  int nz, double dx, double dy, double dz, double* rhs) {
+    OGrid g0 = {nv, nx, ny, nz};
+    const OGrid* g = &g0;
+    const size_t nc = (size_t)nx * ny * nz;
+    const int ng = gr->ng;
+    const double* use = pr;
+    double* copy = NULL;
+    if (gr->orthonormal && (gr->metric == GR_SCHW || gr->metric == GR_KS)) {
+        copy = malloc(sizeof(double) * nv * nc);
+        if (!copy) return -1;
+        memcpy(copy, pr, sizeof(double) * nv * nc);
+        for (int i = ng; i < nx - ng; ++i)
+            for (int j = ng; j < ny - ng; ++j)
+                for (int k = ng; k < nz - ng; ++k) {
+                    double x = (gr->offs_x + (i - ng) + 0.5) * dx;
+                    double y = (j - ng + 0.5) * dy, z = (k - ng + 0.5) * dz;
+                    double alpha, gg[3];
+                    gr_ks(x, y, z, gr->mass, &alpha, gg);
+                    double ax = dmax(alpha, 1e-12);
+                    for (int v = 1; v <= 3; ++v) copy[IX(g, v, i, j, k)] = P(v, i, j, k) / ax;
+                }
+        use = copy;
+    }
+    int rc = oracle_rhs(pa, use, nv, nx, ny, nz, dx, dy, dz, rhs);
+    free(copy);
+    if (rc != 0 || gr->metric == GR_MINK) return rc;
+    const int nr = (pa->physics == 0 ? 5 : 9) + pa->n_passive;
+    OGrid gr_r = {nr, nx, ny, nz};
+    for (int i = ng; i < nx - ng; ++i)
+        for (int j = ng; j < ny - ng; ++j)
+            for (int k = ng; k < nz - ng; ++k) {
+                double x = (gr->offs_x + (i - ng) + 0.5) * dx;
+                double y = (j - ng + 0.5) * dy, z = (k - ng + 0.5) * dz;
+                double gg[3], alpha;
+                if (gr->metric == GR_SCHW) gr_iso(x, y, z, gr->mass, gg);
+                else gr_ks(x, y, z, gr->mass, &alpha, gg);
+                double q[9], U[9];
+                for (int v = 0; v < (pa->physics == 0 ? 5 : 9); ++v) q[v] = P(v, i, j, k);
+                double v2 = q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+                if (v2 >= 1.0) v2 = 1.0 - 1e-14;
+                double W = 1.0 / sqrt(1.0 - v2);
+                double h = 1.0 + pa->gamma / (pa->gamma - 1.0) * q[4] / dmax(q[0], SMALL);
+                double w;
+                if (pa->physics == 0) {
+                    w = q[0] * h * W * W + q[4];
+                    s_p2c(q, U);  /* srhd prim_to_cons: its default gamma 5/3 */
+                } else {
+                    double B2 = q[5] * q[5] + q[6] * q[6] + q[7] * q[7];
+                    w = q[0] * h * W * W + B2 + q[4];
+                    r_p2c(pa, q, U);
+                }
+                rhs[IX(&gr_r, 1, i, j, k)] += w * gg[0];
+                rhs[IX(&gr_r, 2, i, j, k)] += w * gg[1];
+                rhs[IX(&gr_r, 3, i, j, k)] += w * gg[2];
+                rhs[IX(&gr_r, 4, i, j, k)] += U[1] * gg[0] + U[2] * gg[1] + U[3] * gg[2];
+            }
+    return 0;
+}
+
+static int step_impl(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
+                     int nz, double dx, double dy, double dz, double dt, int rk, double* out);
+
 /* One SSPRK2/3 step (srhd_core.py:1286-1400, rmhd_core.py:1559-1677). */
 int oracle_step(const OParams* pa, const double* pr, int nv, int nx, int ny, int nz,
                 double dx, double dy, double dz, double dt, int rk, double* out) {
+    return step_impl(pa, NULL, pr, nv, nx, ny, nz, dx, dy, dz, dt, rk, out);
+}
+
+/* The GR wrappers' steps (grhd_core.py:76-166, grmhd_core.py:80-183): the
+ * core step with the GR right-hand side. */
+int oracle_step_gr(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
+                   int nz, double dx, double dy, double dz, double dt, int rk, double* out) {
+    return step_impl(pa, gr, pr, nv, nx, ny, nz, dx, dy, dz, dt, rk, out);
+}
+
+static int step_impl(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
+                     int nz, double dx, double dy, double dz, double dt, int rk, double* out) {
     const int nm = pa->physics == 0 ? 5 : 9;
     const int np = pa->n_passive, po = pa->passive_offset;
     const size_t nc = (size_t)nx * ny * nz;
@@ -1070,7 +1172,8 @@ int oracle_step(const OParams* pa, const double* pr, int nv, int nx, int ny, int
     const int nst = (rk == 3) ? 3 : 2;
     double* bufs[2] = {prA, prB};
     for (int s = 0; s < nst; ++s) {
-        oracle_rhs(pa, cur, nv, nx, ny, nz, dx, dy, dz, rhs);
+        if (gr) oracle_rhs_gr(pa, gr, cur, nv, nx, ny, nz, dx, dy, dz, rhs);
+        else oracle_rhs(pa, cur, nv, nx, ny, nz, dx, dy, dz, rhs);
         double* dst = (s == nst - 1) ? out : bufs[s % 2];
         memset(dst, 0, sizeof(double) * (size_t)nv * nc);
 #pragma omp parallel for schedule(static)

@@ -28,6 +28,26 @@ class OParams(C.Structure):
                 ("glm_cp", C.c_double), ("resistivity", C.c_double)]
 
 
+class OGR(C.Structure):
+    _fields_ = [("metric", C.c_int), ("orthonormal", C.c_int), ("ng", C.c_int),
+                ("offs_x", C.c_int), ("mass", C.c_double), ("spin", C.c_double)]
+
+
+GR_METRICS = {"minkowski": 0, "schwarzschild": 1, "kerr-schild": 2}
+
+
+def gr_struct(cfg, ng, offs_x):
+    """GR_METRIC / GR_MASS / GR_SPIN / ORTHONORMAL_FLUX as grhd_core.configure
+    reads them (grhd_core.py:13-18); any other metric name goes down the
+    reference's Kerr-Schild source branch without the velocity rescale."""
+    g = OGR()
+    g.metric = GR_METRICS.get(str(cfg.get("GR_METRIC", "minkowski")).lower(), 3)
+    g.orthonormal = 1 if bool(cfg.get("ORTHONORMAL_FLUX", True)) else 0
+    g.ng, g.offs_x = int(ng), int(offs_x)
+    g.mass, g.spin = float(cfg.get("GR_MASS", 1.0)), float(cfg.get("GR_SPIN", 0.0))
+    return g
+
+
 class ONozzle(C.Structure):
     _fields_ = [("ng", C.c_int), ("profile", C.c_int), ("perturb", C.c_int),
                 ("physics", C.c_int), ("b_init", C.c_int), ("n_tracers", C.c_int),
@@ -62,6 +82,11 @@ def lib():
         L.oracle_step.argtypes = [C.POINTER(OParams), dp, C.c_int, C.c_int, C.c_int,
                                   C.c_int, C.c_double, C.c_double, C.c_double,
                                   C.c_double, C.c_int, dp]
+        L.oracle_rhs_gr.argtypes = [C.POINTER(OParams), C.POINTER(OGR), dp, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, dp]
+        L.oracle_step_gr.argtypes = [C.POINTER(OParams), C.POINTER(OGR), dp, C.c_int, C.c_int,
+                                     C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                     C.c_double, C.c_int, dp]
         L.oracle_p2c.argtypes = [C.POINTER(OParams), dp, dp, C.c_long]
         L.oracle_c2p.argtypes = [C.POINTER(OParams), dp, dp, C.c_long]
         L.oracle_c2p_counters.argtypes = [C.POINTER(C.c_long), C.c_int]
@@ -134,6 +159,27 @@ def step(params, pr, dx, dy, dz, dt, rk):
     rc = lib().oracle_step(C.byref(params), _dp(pr), *pr.shape, dx, dy, dz, dt, rk, _dp(out))
     if rc != 0:
         raise RuntimeError(f"oracle_step failed ({rc})")
+    return out
+
+
+def rhs_gr(params, gr, pr, dx, dy, dz):
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    nm = 5 if params.physics == 0 else 9
+    out = np.zeros((nm + params.n_passive,) + pr.shape[1:])
+    rc = lib().oracle_rhs_gr(C.byref(params), C.byref(gr), _dp(pr), *pr.shape, dx, dy, dz,
+                             _dp(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rhs_gr failed ({rc})")
+    return out
+
+
+def step_gr(params, gr, pr, dx, dy, dz, dt, rk):
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    out = np.zeros_like(pr)
+    rc = lib().oracle_step_gr(C.byref(params), C.byref(gr), _dp(pr), *pr.shape, dx, dy, dz, dt,
+                              rk, _dp(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_step_gr failed ({rc})")
     return out
 
 

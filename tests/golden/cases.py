@@ -85,4 +85,36 @@ CASES = [
 
 CASE_BY_NAME = {c["name"]: c for c in CASES}
 
+
+def _gr(name, physics, recon, limiter, riemann, rk, ng, gr, offs_x, seed, **kw):
+    c = _c(name, physics, recon, limiter, riemann, rk, ng, seed=seed, **kw)
+    c.update(gr=gr, offs_x=offs_x)
+    return c
+
+
+# Fixed-metric GR wrappers (core/grhd_core.py, core/grmhd_core.py): black hole
+# of mass 0.05 at the origin, the block's corner next to it (r >= 0.1, lapse
+# >= 0.7), jets at v = 0.5 so that the lapse-rescaled velocities stay below 1
+GR_STATE = dict(vjet=0.5)
+GR_CASES = [
+    _gr("gr_hd_schw_muscl", "srhd", "muscl", "mc", "hlle", 2, 2,
+        dict(GR_METRIC="schwarzschild", GR_MASS=0.05, ORTHONORMAL_FLUX=True), 2, 301,
+        state=GR_STATE, GAMMA=4.0 / 3.0),
+    _gr("gr_hd_ks_ppm_plainflux", "srhd", "ppm", "mc", "hllc", 3, 3,
+        dict(GR_METRIC="kerr-schild", GR_MASS=0.05, ORTHONORMAL_FLUX=False), 0, 302,
+        state=GR_STATE),
+    _gr("gr_hd_other_muscl_pass1", "srhd", "muscl", "vanleer", "hllc", 3, 2,
+        dict(GR_METRIC="isotropic", GR_MASS=0.05, ORTHONORMAL_FLUX=True), 1, 303,
+        n_extra=1, state=GR_STATE),
+    _gr("gr_mhd_schw_weno", "rmhd", "weno", "mc", "hlld", 3, 3,
+        dict(GR_METRIC="schwarzschild", GR_MASS=0.05, ORTHONORMAL_FLUX=True), 1, 304,
+        state=dict(MILD, vjet=0.5)),
+    _gr("gr_mhd_ks_muscl", "rmhd", "muscl", "mc", "hlle", 2, 2,
+        dict(GR_METRIC="kerr-schild", GR_MASS=0.05, ORTHONORMAL_FLUX=True, GR_SPIN=0.5), 3, 305,
+        state=dict(MILD, vjet=0.5)),
+    _gr("gr_mhd_mink_ppm", "rmhd", "ppm", "mc", "hlld", 2, 3,
+        dict(GR_METRIC="minkowski", GR_MASS=0.05), 0, 306, state=dict(MILD, vjet=0.5)),
+]
+GR_BY_NAME = {c["name"]: c for c in GR_CASES}
+
 DT_FRACTION = 0.2  # dt = DT_FRACTION * dx for the single-step fixtures

@@ -23,12 +23,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 import numpy as np  # noqa: E402
-from cases import CASES, CASE_BY_NAME, DT_FRACTION  # noqa: E402
+from cases import CASES, CASE_BY_NAME, DT_FRACTION, GR_CASES, GR_BY_NAME  # noqa: E402
 import states  # noqa: E402
 
 SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
            "c2p_rmhd", "c2p_srhd", "source_terms", "c1_run", "c5_run", "chemistry",
-           "dissipation", "diagnostics"]
+           "dissipation", "diagnostics", "gr_metric"]
 
 NOZZLE_BASE = dict(JET_RADIUS=0.1, SHEAR_THICK=0.02, NOZZLE_PROFILE="top_hat",
                    GAMMA_JET=7.088812050083354, ETA_RHO=0.1, P_EQ=0.01,
@@ -69,6 +69,28 @@ def run_case(name, ref, out):
         extra["max_char_speed"] = np.array(S.max_char_speed(pr, n, n, n))
     np.savez_compressed(out, pr_in=pr, rhs=rhs, step_out=out_pr,
                         dt=np.array(dt), params=json.dumps(p), **extra)
+
+
+def run_gr(name, ref, out):
+    """core/grhd_core.py / core/grmhd_core.py: right-hand side and one step."""
+    S, R, B, N, ST = _import_ref(ref)
+    from core import grhd_core, grmhd_core
+    c = GR_BY_NAME[name]
+    p = c["params"]
+    srhd = c["physics"] == "srhd"
+    (S if srhd else R).configure(p)
+    G = grhd_core if srhd else grmhd_core
+    G.configure(c["gr"])
+    pr = states.make_state(c["seed"], c["n"], c["ng"], c["physics"],
+                           c["n_extra"] + c["pad"], **c["state"])
+    dx = 1.0 / c["n"]
+    rhs_fn = G.compute_rhs_grhd if srhd else G.compute_rhs_grmhd
+    rhs = rhs_fn(pr, dx, dx, dx, c["offs_x"], c["ng"])
+    dt = DT_FRACTION * dx
+    step = G.step_ssprk3 if c["rk"] == 3 else G.step_ssprk2
+    out_pr = step(pr.copy(), dx, dx, dx, dt, c["offs_x"], c["ng"])
+    np.savez_compressed(out, pr_in=pr, rhs=rhs, step_out=out_pr, dt=np.array(dt),
+                        params=json.dumps(p), gr=json.dumps(c["gr"]))
 
 
 def _bc_setup(name):
@@ -387,6 +409,19 @@ def one(name, ref):
         run_chem_dissip(name, ref, out)
     elif name == "diagnostics":
         run_diagnostics(name, ref, out)
+    elif name in GR_BY_NAME:
+        run_gr(name, ref, out)
+    elif name == "gr_metric":
+        sys.path.insert(0, ref)
+        from core import gr_metric as GM
+        pts = np.random.default_rng(707).uniform(-2.0, 2.0, (64, 3))
+        pts[0] = 0.0  # the 1e-12 offset of r
+        pts[1] = (0.025, 0.0, 0.0)  # r = M/2 for M = 0.05: 1 - a^2 = 0 branch
+        iso = [GM.schwarzschild_iso_lapse_and_grad(*p, 0.05) for p in pts]
+        ks = [GM.schwarzschild_ks_lapse_shift_and_grad(*p, 0.05) for p in pts]
+        kerr = [GM.kerr_schild_lapse_shift_and_grad(*p, 0.05, 0.7) for p in pts]
+        np.savez_compressed(out, pts=pts, iso=np.array(iso), ks=np.array(ks),
+                            kerr=np.array(kerr))
     else:
         run_loop(name, ref, out)
     print("wrote", out, flush=True)
@@ -402,7 +437,7 @@ def main():
     if a.one:
         one(a.one, a.ref)
         return
-    names = a.names or ([c["name"] for c in CASES] + SPECIAL)
+    names = a.names or ([c["name"] for c in CASES] + SPECIAL + [c["name"] for c in GR_CASES])
     env = dict(os.environ, PYTHONDONTWRITEBYTECODE="1", NUMBA_NUM_THREADS="1")
 
     def launch(nm):
