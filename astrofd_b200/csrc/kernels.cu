@@ -560,17 +560,21 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 6) k_update(UpdArg
 // Five invariants of a conserved RMHD state (log D, |S|/D, tau/D, B^2/D,
 // (S.B)^2/D^3), the last four through log1p so the inputs stay O(1).
 __device__ __forceinline__ void c2p_features(const double* U, float* x) {
-    const double D = rmax(U[0], 1e-300);
     const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
     const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
     const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
-    const double iD = 1.0 / D;
-    const double r[4] = {sqrt(S2) * iD, rmax(U[4], 0.0) * iD, B2 * iD, SB * SB * iD * iD * iD};
-    // the features feed a bfloat16 network (8-bit mantissa): the fast
-    // float32 logarithm (one MUFU operation) is far more accurate than that
-    x[0] = __logf((float)rmax(D, 1e-30));
+    // the features feed a bfloat16 network (8-bit mantissa): the ratios in
+    // float32 with the approximate reciprocal and square root, and the fast
+    // float32 logarithm (one MUFU operation each), are far more accurate than
+    // that; overflowing ratios saturate at the 1e30 clamp
+    const float Df = fminf(fmaxf((float)U[0], 1e-30f), 1e30f);
+    const float iD = rcp_(Df);
+    const float sb = (float)SB * iD;
+    const float r[4] = {sqrtf((float)S2) * iD, fmaxf((float)U[4], 0.f) * iD, (float)B2 * iD,
+                        sb * sb * iD};
+    x[0] = __logf(Df);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) x[1 + i] = __logf(1.0f + (float)rmin(r[i], 1e30));
+    for (int i = 0; i < 4; ++i) x[1 + i] = __logf(1.0f + fminf(r[i], 1e30f));
 }
 
 struct C2PArgs {

@@ -335,7 +335,7 @@ __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, u
 
 __device__ __forceinline__ void features_norm(const Params* P, const float* xr, float* h0) {
 #pragma unroll
-    for (int i = 0; i < NIN; ++i) h0[i] = (xr[i] - P->xmu[i]) / P->xsd[i];
+    for (int i = 0; i < NIN; ++i) h0[i] = __fdividef(xr[i] - P->xmu[i], P->xsd[i]);
 }
 
 }  // namespace mlp

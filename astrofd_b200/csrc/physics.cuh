@@ -810,35 +810,40 @@ AHD void r_c2p_start(const Phys<double>& P, const double* U, double* q0, double&
 // clamped quantity is constant and contributes nothing.
 AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
                        double SB, double S2, double* df) {
+    // the reference's divisions regrouped around four quotients (1/Z,
+    // 1/(Z+B^2)^2, 1/(1-v^2), Z/(rho W^2)) and one square root: the same
+    // residual to rounding, far inside the Newton tolerance
     const double G = P.gamma, SM = 1e-12;
-    const double denomZ = rmax(Z, SM);
-    const double vb = SB / denomZ;
+    const double iZ = 1.0 / rmax(Z, SM);
+    const double vb = SB * iZ;
     const double ZpB = Z + B2;
     const double Bq = ZpB * ZpB + SM;
-    double v2 = (S2 + (SB * SB) * (2.0 * Z + B2) / (denomZ * denomZ)) / Bq;
+    const double iBq = 1.0 / Bq;
+    double v2 = (S2 + (SB * SB) * (2.0 * Z + B2) * (iZ * iZ)) * iBq;
     const double vmax2 = P.v_max * P.v_max;
     const bool vcap = v2 >= vmax2;
     if (vcap) v2 = vmax2 - 1e-14;
-    const double W2 = 1.0 / (1.0 - v2);
-    const double W = sqrt(W2);
-    const double rho = D / rmax(W, SM);
+    const double om = 1.0 - v2;  // 1 / W^2
+    const double W2 = 1.0 / om;
+    const double rho = D * sqrt(om);  // D / W, W >= 1
     const double h = Z / rmax(rho * W2, SM);
-    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    const double gm = (G - 1.0) / G;
+    double p = (h - 1.0) * rho * gm;
     bool pcap = false;
     if (p < SM) { p = SM; pcap = true; }
     if (p > P.p_max) { p = P.p_max; pcap = true; }
-    const double b2 = B2 / W2 + vb * vb;
+    const double b2 = B2 * om + vb * vb;
     const double f = (Z - p + 0.5 * B2 + 0.5 * b2 - D) - tau;
     if (df) {
         const bool zfloor = Z < SM;
-        const double iZ = 1.0 / denomZ;
-        const double dA = zfloor ? 0.0 : -2.0 * SB * SB * ZpB * iZ * iZ * iZ;
-        const double dv2 = vcap ? 0.0 : (dA - v2 * 2.0 * ZpB) / Bq;
+        const double dA = zfloor ? 0.0 : -2.0 * SB * SB * ZpB * (iZ * iZ * iZ);
+        const double dv2 = vcap ? 0.0 : (dA - v2 * 2.0 * ZpB) * iBq;
         const double dW2 = W2 * W2 * dv2;
-        const double drho = -0.5 * rho * dW2 / W2;  // rho = D W2^-1/2
-        const double dp = pcap ? 0.0 : (G - 1.0) / G * (1.0 / W2 - Z * dW2 / (W2 * W2) - drho);
+        const double om2 = om * om;
+        const double drho = -0.5 * rho * dW2 * om;  // rho = D W2^-1/2
+        const double dp = pcap ? 0.0 : gm * (om - Z * dW2 * om2 - drho);
         const double dvb = zfloor ? 0.0 : -vb * iZ;
-        const double db2 = -B2 * dW2 / (W2 * W2) + 2.0 * vb * dvb;
+        const double db2 = -B2 * dW2 * om2 + 2.0 * vb * dvb;
         *df = 1.0 - dp + 0.5 * db2;
     }
     return f;
@@ -882,21 +887,23 @@ AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U
     double Bx = U[5], By = U[6], Bz = U[7];
     double B2 = Bx * Bx + By * By + Bz * Bz;
     double SB = Sx * Bx + Sy * By + Sz * Bz;
+    // divisions regrouped as in r_f_df_of_Z (same values to rounding)
     double ZpB = Z + B2;
-    double vb = SB / rmax(Z, SM);
-    double vx = (Sx + vb * Bx) / rmax(ZpB, SM);
-    double vy = (Sy + vb * By) / rmax(ZpB, SM);
-    double vz = (Sz + vb * Bz) / rmax(ZpB, SM);
+    double vb = SB * (1.0 / rmax(Z, SM));
+    const double iZB = 1.0 / rmax(ZpB, SM);
+    double vx = (Sx + vb * Bx) * iZB;
+    double vy = (Sy + vb * By) * iZB;
+    double vz = (Sz + vb * Bz) * iZB;
     double v2 = vx * vx + vy * vy + vz * vz;
     double vmax2 = P.v_max * P.v_max;
     if (v2 >= vmax2) {
         double fac = P.v_max / sqrt(v2 + 1e-32);
         vx *= fac; vy *= fac; vz *= fac;
     }
-    double W = 1.0 / sqrt(1.0 - (vx * vx + vy * vy + vz * vz));
-    double rho = D / rmax(W, SM);
-    double h = Z / rmax(rho * W * W, SM);
-    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    const double om = 1.0 - (vx * vx + vy * vy + vz * vz);  // 1 / W^2
+    double rho = D * sqrt(om);                               // D / W, W >= 1
+    double h = Z / rmax(rho / om, SM);
+    double p = (h - 1.0) * rho * ((G - 1.0) / G);
     if (!isfinite(rho) || !isfinite(p) || rho <= 0.0 || p <= 0.0) return false;
     q[0] = rho; q[1] = vx; q[2] = vy; q[3] = vz; q[4] = p;
     q[5] = Bx; q[6] = By; q[7] = Bz; q[8] = U[8];
