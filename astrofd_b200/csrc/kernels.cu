@@ -268,18 +268,20 @@ __device__ __forceinline__ bool face_at(const FaceArgs& a, int i, int j, int k) 
 
 template <int PHYS, int RECON, int RIEMANN, typename R, bool GIVEN, int DIR>
 __global__ void __launch_bounds__(128) k_face(FaceArgs a) {
-    const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const int c = (int)(t % a.ext[2]);
-    const long r = t / a.ext[2];
-    const int bb = (int)(r % a.ext[1]);
-    const int aa = (int)(r / a.ext[1]);
-    const int i = a.org[0] + aa, j = a.org[1] + bb, k = a.org[2] + c;
-    const bool ok = face_at<PHYS, RECON, RIEMANN, R, R, GIVEN, DIR>(a, i, j, k);
-    if (sizeof(R) == 4 && !ok && a.fix_list) {
-        const unsigned slot = atomicAdd(a.fix_count, 1u);
-        if (slot < a.fix_cap) a.fix_list[slot] = (unsigned)t;
+    // grid: x over the (j, k) plane of the face block, y over its x layers;
+    // one 32-bit split of the in-plane index per thread
+    const unsigned e2 = (unsigned)a.ext[2];
+    const unsigned plane = (unsigned)a.ext[1] * e2;
+    const unsigned tp = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tp >= plane) return;
+    const int c = (int)(tp % e2), bb = (int)(tp / e2);
+    for (int aa = blockIdx.y; aa < a.ext[0]; aa += gridDim.y) {
+        const int i = a.org[0] + aa, j = a.org[1] + bb, k = a.org[2] + c;
+        const bool ok = face_at<PHYS, RECON, RIEMANN, R, R, GIVEN, DIR>(a, i, j, k);
+        if (sizeof(R) == 4 && !ok && a.fix_list) {
+            const unsigned slot = atomicAdd(a.fix_count, 1u);
+            if (slot < a.fix_cap) a.fix_list[slot] = (unsigned)aa * plane + tp;
+        }
     }
 }
 
@@ -823,7 +825,8 @@ template <typename R>
 cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
     const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
     if (total <= 0) return cudaSuccess;
-    const dim3 blk(128), grd((unsigned)((total + 127) / 128));
+    const unsigned plane = (unsigned)a.ext[1] * (unsigned)a.ext[2];
+    const dim3 blk(128), grd((plane + 127) / 128, (unsigned)(a.ext[0] < 65535 ? a.ext[0] : 65535));
     const AstroParams& p = a.p;
 #define FACE(PH, RE, RI) launch_face_dir<PH, RE, RI, R>(a, given, grd, blk, s)
 #define RECONS(PH, RI)                                                          \
