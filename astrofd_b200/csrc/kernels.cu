@@ -616,7 +616,7 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     if (net) {
         if (t < 32) mlp::tmem_alloc(mlp::smem_u32(taddr_s), 64);
         if (t == 0) mlp::mbar_init_fenced(mlp::smem_u32(bar), 1);
-        mlp::load_weights(sm, a.net);
+        mlp::load_weights(sm, a.net, true);
         mlp::fence_async_smem();
         mlp::tc_fence_before();
     }

@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const Params* P, const floa
     const int t = threadIdx.x;
     if (t < 32) tmem_alloc(smem_u32(taddr_s), 64);
     if (t == 0) mbar_init_fenced(smem_u32(bar), 1);
-    load_weights(sm, P);
+    load_weights(sm, P, true);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();

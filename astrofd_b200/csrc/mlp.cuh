@@ -202,13 +202,15 @@ __device__ __forceinline__ float silu_grad(float z) {
 }
 
 // SiLU of 16 accumulator columns after adding their biases, two columns per
-// packed float32x2 instruction (sm_100 FADD2/FMUL2/FFMA2)
-__device__ __forceinline__ void bias_silu16(const float* z, const float* bias, float* h) {
+// packed float32x2 instruction (sm_100 FADD2/FFMA2).  The inference weights
+// and biases of layers 1-3 are stored halved (load_weights(.., true)): scaling
+// by 2 commutes with every rounding of the MMA and the bias add, so the sum is
+// exactly h = z/2 and SiLU(z) = h + h tanh(h) needs no multiply.
+__device__ __forceinline__ void bias_silu16(const float* z, const float* bias_half, float* h) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const float2 b = *reinterpret_cast<const float2*>(bias + 2 * i);
-        const float2 zz = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]), b);
-        const float2 hh = __fmul2_rn(zz, make_float2(0.5f, 0.5f));
+        const float2 b = *reinterpret_cast<const float2*>(bias_half + 2 * i);
+        const float2 hh = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]), b);
         const float2 tt = make_float2(tanh_approx(hh.x), tanh_approx(hh.y));
         const float2 ss = __ffma2_rn(hh, tt, hh);
         h[2 * i] = ss.x;
@@ -224,19 +226,22 @@ __device__ __forceinline__ void st_row8(unsigned char* base, int R, int r, int c
     *reinterpret_cast<uint4*>(base + elem_off(R, r, c0)) = *reinterpret_cast<uint4*>(p);
 }
 
-// FP32 master weights -> bf16 K-major operands in shared memory (all threads)
-__device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P) {
+// FP32 master weights -> bf16 K-major operands in shared memory (all
+// threads).  halve: layers 1-3 and their biases at half scale (exact in bf16
+// and float32), for the inference epilogue bias_silu16.
+__device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P, bool halve = false) {
+    const float hs = halve ? 0.5f : 1.0f;
     for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {  // W1 [64 x 16], in 5..15 = 0
         int o = e / 16, i = e % 16;
         float w = i < NIN ? P->W1[o * NIN + i] : 0.f;
-        *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W1 + elem_off(64, o, i)) = __float2bfloat16_rn(w);
+        *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W1 + elem_off(64, o, i)) = __float2bfloat16_rn(hs * w);
     }
     for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
         int o = e / 64, i = e % 64;
         *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W2 + elem_off(64, o, i)) =
-            __float2bfloat16_rn(P->W2[o * H + i]);
+            __float2bfloat16_rn(hs * P->W2[o * H + i]);
         *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W3 + elem_off(64, o, i)) =
-            __float2bfloat16_rn(P->W3[o * H + i]);
+            __float2bfloat16_rn(hs * P->W3[o * H + i]);
     }
     for (int e = threadIdx.x; e < 16 * 64; e += blockDim.x) {  // W4 [16 x 64], rows 2..15 = 0
         int o = e / 64, i = e % 64;
@@ -245,7 +250,9 @@ __device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P)
     }
     float* bs = reinterpret_cast<float*>(sm + OFF_BIAS);
     for (int e = threadIdx.x; e < 3 * H + NOUT; e += blockDim.x)
-        bs[e] = e < H ? P->b1[e] : (e < 2 * H ? P->b2[e - H] : (e < 3 * H ? P->b3[e - 2 * H] : P->b4[e - 3 * H]));
+        bs[e] = e < H ? hs * P->b1[e]
+                      : (e < 2 * H ? hs * P->b2[e - H]
+                                   : (e < 3 * H ? hs * P->b3[e - 2 * H] : P->b4[e - 3 * H]));
 }
 
 // Issue D[128 x N] (+)= A[128 x K] . B for K = 16*ksteps, both operands
@@ -263,7 +270,8 @@ __device__ __forceinline__ void mma_kmajor(uint32_t tmem_d, uint32_t a_addr, int
 
 // forward pass of one tile, in shared memory / TMEM.  Thread t owns row t.
 // h0: normalised features of this thread's row.  When TRAIN, keeps H1..H3 and
-// SiLU'(z) for the backward pass; otherwise H1 is reused for every layer.
+// SiLU'(z) for the backward pass; otherwise H1 is reused for every layer and
+// the weights are the halved ones of load_weights(.., true).
 // Returns false if an MMA wait timed out (uniform across the block).
 template <bool TRAIN>
 __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, uint32_t mbar, uint32_t& phase,

@@ -158,9 +158,9 @@ __device__ __forceinline__ float2 weno5_pair(const float* s) {
     const float2 t2 = __fadd2_rn(__ffma2_rn(D, m2, Cc), E);
     const float2 u2 = __fadd2_rn(__ffma2_rn(D, k2(-4.f), __fmul2_rn(Cc, k2(3.f))), E);
     const float2 c13 = k2(13.f / 12.f), q = k2(0.25f), eps = k2(1e-12f);
-    const float2 w0 = __fadd2_rn(__ffma2_rn(__fmul2_rn(t0, c13), t0, __fmul2_rn(__fmul2_rn(u0, q), u0)), eps);
-    const float2 w1 = __fadd2_rn(__ffma2_rn(__fmul2_rn(t1, c13), t1, __fmul2_rn(__fmul2_rn(u1, q), u1)), eps);
-    const float2 w2 = __fadd2_rn(__ffma2_rn(__fmul2_rn(t2, c13), t2, __fmul2_rn(__fmul2_rn(u2, q), u2)), eps);
+    const float2 w0 = __ffma2_rn(__fmul2_rn(t0, c13), t0, __ffma2_rn(__fmul2_rn(u0, q), u0, eps));
+    const float2 w1 = __ffma2_rn(__fmul2_rn(t1, c13), t1, __ffma2_rn(__fmul2_rn(u1, q), u1, eps));
+    const float2 w2 = __ffma2_rn(__fmul2_rn(t2, c13), t2, __ffma2_rn(__fmul2_rn(u2, q), u2, eps));
     const float2 v0 = __fmul2_rn(w0, w0), v1 = __fmul2_rn(w1, w1), v2 = __fmul2_rn(w2, w2);
     const float2 a0 = __fmul2_rn(make_float2(rcp_(v0.x), rcp_(v0.y)), k2(0.1f));
     const float2 a1 = __fmul2_rn(make_float2(rcp_(v1.x), rcp_(v1.y)), k2(0.6f));
