@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
             // long solves do not hold up the 31 other cells of this warp
             if (c2p_defer(a, cell)) continue;
         }
-        if (!done) r_c2p(P, U, q, cnt);
+        if (!done) r_c2p<true>(P, U, q, cnt);
 #pragma unroll
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
         if (a.qf)
@@ -711,7 +711,7 @@ __global__ void __launch_bounds__(128) k_c2p_fallback(C2PArgs a) {
         double U[9], q[9];
 #pragma unroll
         for (int v = 0; v < 9; ++v) U[v] = a.U[(size_t)v * a.count + cell];
-        r_c2p(P, U, q, cnt);
+        r_c2p<true>(P, U, q, cnt);
 #pragma unroll
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
         if (a.qf)

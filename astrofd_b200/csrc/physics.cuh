@@ -681,6 +681,9 @@ AHD void r_c2p_hydro(const Phys<double>& P, double D, double Sx, double Sy, doub
     s_c2p(Q, U, q);
 }
 
+AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
+                       double SB, double S2, double* df);
+
 AHD double r_f_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
                     double SB, double S2) {
     const double G = P.gamma, SM = 1e-12;
@@ -702,20 +705,33 @@ AHD double r_f_of_Z(const Phys<double>& P, double Z, double D, double tau, doubl
     return tau_calc - tau;
 }
 
+// f(Z) in the reference's operation order (float64 reference mode), or
+// (FAST) the same expressions with the divisions regrouped (r_f_df_of_Z):
+// equal to rounding, with a dependency chain about half as long, for the
+// learned path's fallback solves, whose time is the latency of its slowest
+// cells
+template <bool FAST>
+AHD double r_f_eval(const Phys<double>& P, double Z, double D, double tau, double B2,
+                    double SB, double S2) {
+    if constexpr (FAST) return r_f_df_of_Z(P, Z, D, tau, B2, SB, S2, nullptr);
+    else return r_f_of_Z(P, Z, D, tau, B2, SB, S2);
+}
+
 // The reference's Newton on Z from a starting value: up to 50 steps with the
 // forward-difference derivative and +-Z/2 step clamp (rmhd_core.py:268-292).
 // Returns true when |f| < 1e-10 max(1, tau).
+template <bool FAST = false>
 AHD bool r_newton(const Phys<double>& P, double& Z, int max_it, double D, double tau,
                   double B2, double SB, double S2, int* steps = nullptr) {
     const double tol = 1e-10 * rmax(1.0, tau);
     for (int it = 0; it < max_it; ++it) {
-        double f = r_f_of_Z(P, Z, D, tau, B2, SB, S2);
+        double f = r_f_eval<FAST>(P, Z, D, tau, B2, SB, S2);
         if (fabs(f) < tol) {
             if (steps) *steps = it;
             return true;
         }
         double eps = 1e-6 * rmax(1.0, Z);
-        double fp = r_f_of_Z(P, Z + eps, D, tau, B2, SB, S2);
+        double fp = r_f_eval<FAST>(P, Z + eps, D, tau, B2, SB, S2);
         double dfdZ = (fp - f) / eps;
         if (dfdZ == 0.0) break;
         double dZ = -f / dfdZ;
@@ -728,7 +744,9 @@ AHD bool r_newton(const Phys<double>& P, double& Z, int max_it, double D, double
     return false;
 }
 
-// Primitive recovery once Z is known (rmhd_core.py:320-341)
+// Primitive recovery once Z is known (rmhd_core.py:320-341); FAST as in
+// r_f_eval
+template <bool FAST = false>
 AHD void r_prims_from_Z(const Phys<double>& P, double Z, const double* U, const double* q0,
                         double* q, C2PCount& cnt) {
     const double G = P.gamma, SM = 1e-12;
@@ -737,20 +755,36 @@ AHD void r_prims_from_Z(const Phys<double>& P, double Z, const double* U, const 
     double B2 = Bx * Bx + By * By + Bz * Bz;
     double SB = Sx * Bx + Sy * By + Sz * Bz;
     double ZpB = Z + B2;
-    double vb = SB / rmax(Z, SM);
-    double vx = (Sx + vb * Bx) / rmax(ZpB, SM);
-    double vy = (Sy + vb * By) / rmax(ZpB, SM);
-    double vz = (Sz + vb * Bz) / rmax(ZpB, SM);
+    double vx, vy, vz, rho, h, p;
+    if constexpr (FAST) {
+        const double vb = SB * (1.0 / rmax(Z, SM));
+        const double iZB = 1.0 / rmax(ZpB, SM);
+        vx = (Sx + vb * Bx) * iZB;
+        vy = (Sy + vb * By) * iZB;
+        vz = (Sz + vb * Bz) * iZB;
+    } else {
+        double vb = SB / rmax(Z, SM);
+        vx = (Sx + vb * Bx) / rmax(ZpB, SM);
+        vy = (Sy + vb * By) / rmax(ZpB, SM);
+        vz = (Sz + vb * Bz) / rmax(ZpB, SM);
+    }
     double v2 = vx * vx + vy * vy + vz * vz;
     double vmax2 = P.v_max * P.v_max;
     if (v2 >= vmax2) {
         double fac = P.v_max / sqrt(v2 + 1e-32);
         vx *= fac; vy *= fac; vz *= fac;
     }
-    double W = 1.0 / sqrt(1.0 - (vx * vx + vy * vy + vz * vz));
-    double rho = D / rmax(W, SM);
-    double h = Z / rmax(rho * W * W, SM);
-    double p = (h - 1.0) * rho * (G - 1.0) / G;
+    if constexpr (FAST) {
+        const double om = 1.0 - (vx * vx + vy * vy + vz * vz);
+        rho = D * sqrt(om);
+        h = Z / rmax(rho / om, SM);
+        p = (h - 1.0) * rho * ((G - 1.0) / G);
+    } else {
+        double W = 1.0 / sqrt(1.0 - (vx * vx + vy * vy + vz * vz));
+        rho = D / rmax(W, SM);
+        h = Z / rmax(rho * W * W, SM);
+        p = (h - 1.0) * rho * (G - 1.0) / G;
+    }
     if (!isfinite(rho) || !isfinite(p) || rho <= 0.0 || p <= 0.0) {
         cnt.hydro_fallback++;
         rho = q0[0]; vx = q0[1]; vy = q0[2]; vz = q0[3]; p = q0[4];
@@ -761,22 +795,23 @@ AHD void r_prims_from_Z(const Phys<double>& P, double Z, const double* U, const 
 }
 
 // Bisection fallback (rmhd_core.py:294-318); Z holds the last Newton iterate
+template <bool FAST = false>
 AHD void r_bisect(const Phys<double>& P, double& Z, double Z1, double D, double tau, double B2,
                   double SB, double S2) {
     double Zmin = 1e-12;
     double Zmax = rmax(rmax(Z, Z1), 1.0);
-    double fmin = r_f_of_Z(P, Zmin, D, tau, B2, SB, S2);
-    double fmax = r_f_of_Z(P, Zmax, D, tau, B2, SB, S2);
+    double fmin = r_f_eval<FAST>(P, Zmin, D, tau, B2, SB, S2);
+    double fmax = r_f_eval<FAST>(P, Zmax, D, tau, B2, SB, S2);
     for (int it = 0; it < 40; ++it) {
         if (fmin * fmax <= 0.0) break;
         Zmax *= 2.0;
-        fmax = r_f_of_Z(P, Zmax, D, tau, B2, SB, S2);
+        fmax = r_f_eval<FAST>(P, Zmax, D, tau, B2, SB, S2);
     }
     if (fmin * fmax <= 0.0) {
         const double tol = 1e-10 * rmax(1.0, tau);
         for (int it = 0; it < 60; ++it) {
             double Zmid = 0.5 * (Zmin + Zmax);
-            double fmid = r_f_of_Z(P, Zmid, D, tau, B2, SB, S2);
+            double fmid = r_f_eval<FAST>(P, Zmid, D, tau, B2, SB, S2);
             if (fabs(fmid) < tol) { Z = Zmid; break; }
             if (fmin * fmid <= 0.0) { Zmax = Zmid; fmax = fmid; }
             else { Zmin = Zmid; fmin = fmid; }
@@ -911,7 +946,10 @@ AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U
     return true;
 }
 
-// Full reference con2prim (cons_to_prim_rmhd, rmhd_core.py:249-341)
+// Full reference con2prim (cons_to_prim_rmhd, rmhd_core.py:249-341); FAST:
+// its f(Z) and primitive recovery with the regrouped divisions (the learned
+// path's fallback), otherwise the reference's operation order
+template <bool FAST = false>
 AHD void r_c2p(const Phys<double>& P, const double* U, double* q, C2PCount& cnt) {
     double D = U[0], tau = U[4];
     double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
@@ -920,17 +958,17 @@ AHD void r_c2p(const Phys<double>& P, const double* U, double* q, C2PCount& cnt)
     double q0[5], Z0, Z1;
     r_c2p_start(P, U, q0, Z0, Z1);
     double Z = Z0;
-    bool ok = r_newton(P, Z, 50, D, tau, B2, SB, S2);
+    bool ok = r_newton<FAST>(P, Z, 50, D, tau, B2, SB, S2);
     if (!ok) {
         Z = Z1;
-        ok = r_newton(P, Z, 50, D, tau, B2, SB, S2);
+        ok = r_newton<FAST>(P, Z, 50, D, tau, B2, SB, S2);
     }
     if (ok) cnt.newton++;
     else {
         cnt.bisect++;
-        r_bisect(P, Z, Z1, D, tau, B2, SB, S2);
+        r_bisect<FAST>(P, Z, Z1, D, tau, B2, SB, S2);
     }
-    r_prims_from_Z(P, Z, U, q0, q, cnt);
+    r_prims_from_Z<FAST>(P, Z, U, q0, q, cnt);
 }
 
 }  // namespace astro
