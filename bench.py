@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
                     help="with --gpus N > 1: x-slabs of one jet with a ghost exchange per "
                          "step, or N independent blocks")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch every kernel of the timed steps from the host instead of "
+                         "replaying CUDA graphs of one driver iteration")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -242,8 +245,29 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     b = torch.empty_like(a)
     for _ in range(args.warmup):
         a, b, _ = step(a, b)
-    rmhd_core.c2p_stats(reset=True)
     L = _lib.load()
+    # one driver iteration is a fixed sequence of kernels on fixed buffers (no
+    # host-drawn nozzle perturbation in this workload): capture a -> b and
+    # b -> a as CUDA graphs and replay them, which removes the launch gaps
+    # between the ~30 kernels of a step.  Slab runs (NCCL exchange in the
+    # step) launch eagerly.
+    graphs, per_iter, graph_note = None, 0, "eager launches"
+    if not args.no_graph and step.slab is None:
+        try:
+            torch.cuda.synchronize()
+            g1, g2 = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+            l0 = L.astro_launch_count()
+            with torch.cuda.graph(g1):
+                step(a, b)
+            per_iter = L.astro_launch_count() - l0
+            with torch.cuda.graph(g2):
+                step(b, a)
+            graphs = (g1, g2)
+            graph_note = f"CUDA graphs of one driver iteration ({per_iter} kernels), replayed"
+        except Exception as e:  # capture unsupported here: time eager launches
+            graphs, graph_note = None, f"eager launches (graph capture failed: {e})"[:200]
+            torch.cuda.synchronize()
+    rmhd_core.c2p_stats(reset=True)
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     prof_ms = np.zeros(5)
@@ -253,12 +277,16 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     l0 = L.astro_launch_count()
     with ClockSampler(torch.cuda.current_device()) as clk:
         e0.record(stream)
-        for _ in range(args.steps):
-            a, b, _ = step(a, b)
+        for i in range(args.steps):
+            if graphs is not None:
+                graphs[i % 2].replay()
+                a, b = b, a
+            else:
+                a, b, _ = step(a, b)
         e1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
-    launches = L.astro_launch_count() - l0
+    launches = (L.astro_launch_count() - l0) if graphs is None else per_iter * args.steps
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     finite = bool(torch.isfinite(a).all().item())
     stats = rmhd_core.c2p_stats(reset=True)
@@ -271,9 +299,11 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
         a, b, t = step(a, b, profile=True)
         prof_ms += np.array(t[0])
         prof_n += np.array(t[1])
+    if graphs is not None:
+        del graphs
     return dict(ms=ms, launches=int(launches), prof_ms=prof_ms, prof_n=prof_n,
                 prof_steps=prof_steps, clocks=clk.summary(), finite=finite, state=state,
-                c2p=stats)
+                c2p=stats, launch_mode=graph_note)
 
 
 def time_e2e(args, world, prec, pr_host, cfgs, learned=False):
@@ -683,6 +713,7 @@ def main():
                                    "(NCCL send/recv)" if args.decomp == "slab" else
                                    f"replicas x{world}")},
         "gpu_launches": mixed["launches"],
+        "launch_mode": mixed["launch_mode"],
         "clocks": mixed["clocks"],
         "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed", learned),
         "kernel_ms_per_step": {k: round(mixed["prof_ms"][c] / mixed["prof_steps"], 3)
