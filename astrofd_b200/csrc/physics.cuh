@@ -383,7 +383,11 @@ AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR, int n
 }
 
 // ----------------------------------------------------------------- RMHD ---
-template <typename R> AHD void r_p2c(const Phys<R>& P, const R* qin, R* U) {
+// rhoh_out / b2_out: rho h and b^2 of the state, for the fast speed of the
+// same (floored) state on the float32 faces
+template <typename R>
+AHD void r_p2c(const Phys<R>& P, const R* qin, R* U, R* rhoh_out = nullptr,
+               R* b2_out = nullptr) {
     const R gamma = P.gamma;
     R rho = qin[0], vx = qin[1], vy = qin[2], vz = qin[3], p = qin[4];
     R Bx = qin[5], By = qin[6], Bz = qin[7];
@@ -422,6 +426,8 @@ template <typename R> AHD void r_p2c(const Phys<R>& P, const R* qin, R* U) {
     U[3] = wtot * vz - (Bz * vb);
     U[4] = rhohW2 - p + R(0.5) * B2 + R(0.5) * b2 - D;
     U[5] = Bx; U[6] = By; U[7] = Bz; U[8] = qin[8];
+    if (rhoh_out) *rhoh_out = rhoh;
+    if (b2_out) *b2_out = b2;
 }
 
 // physical flux from primitives q and U = p2c(q) (flux_rmhd_x/y/z,
@@ -446,6 +452,25 @@ template <typename R> AHD void r_flux(const Phys<R>& P, int n, const R* q, R* F)
     R U[9];
     r_p2c(P, q, U);
     r_flux_u(P, n, q, U, F);
+}
+
+// fast magnetosonic speed from rho h and b^2 (rmhd_fast_speed,
+// rmhd_core.py:420-458, after its b-vector)
+template <typename R> AHD R r_fast_speed_from(const Phys<R>& P, R p, R rhoh, R b2) {
+    const R G = P.gamma;
+    R cs2 = qdiv(G * p, rmax(rhoh, C<R>::small));
+    if (cs2 < R(0)) cs2 = R(0);
+    if (cs2 > R(1) - R(1e-14)) cs2 = R(1) - R(1e-14);
+    R ca2 = qdiv(b2, rmax(rhoh + b2, C<R>::small));
+    if (ca2 < R(0)) ca2 = R(0);
+    if (ca2 > R(1) - R(1e-14)) ca2 = R(1) - R(1e-14);
+    R a = cs2 + ca2 - cs2 * ca2;
+    R disc = a * a - R(4) * cs2 * ca2;
+    if (disc < R(0)) disc = R(0);
+    R cf2 = R(0.5) * (a + rsqrt_(disc));
+    if (cf2 < R(0)) cf2 = R(0);
+    if (cf2 > R(1) - R(1e-14)) cf2 = R(1) - R(1e-14);
+    return rsqrt_(cf2);
 }
 
 template <typename R> AHD R r_fast_speed(const Phys<R>& P, const R* q) {
@@ -473,19 +498,7 @@ template <typename R> AHD R r_fast_speed(const Phys<R>& P, const R* q) {
     }
     R b0 = W * vb;
     R b2 = (bx * bx + by * by + bz * bz) - b0 * b0;
-    R cs2 = qdiv(G * p, rmax(rhoh, C<R>::small));
-    if (cs2 < R(0)) cs2 = R(0);
-    if (cs2 > R(1) - R(1e-14)) cs2 = R(1) - R(1e-14);
-    R ca2 = qdiv(b2, rmax(rhoh + b2, C<R>::small));
-    if (ca2 < R(0)) ca2 = R(0);
-    if (ca2 > R(1) - R(1e-14)) ca2 = R(1) - R(1e-14);
-    R a = cs2 + ca2 - cs2 * ca2;
-    R disc = a * a - R(4) * cs2 * ca2;
-    if (disc < R(0)) disc = R(0);
-    R cf2 = R(0.5) * (a + rsqrt_(disc));
-    if (cf2 < R(0)) cf2 = R(0);
-    if (cf2 > R(1) - R(1e-14)) cf2 = R(1) - R(1e-14);
-    return rsqrt_(cf2);
+    return r_fast_speed_from(P, p, rhoh, b2);
 }
 
 // hll_d_flux_dir (rmhd_core.py:602-724): approximate HLLD, HLLE on degenerate states
@@ -610,11 +623,28 @@ AHD void r_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
     R UL[9], UR[9], FL[9], FR[9];
     floor_prim(P, qL);
     floor_prim(P, qR);
-    r_p2c(P, qL, UL);
-    r_p2c(P, qR, UR);
-    r_flux_u(P, n, qL, UL, FL);
-    r_flux_u(P, n, qR, UR, FR);
-    if (!GIVEN) r_speeds(P, n, qL, qR, sL, sR);
+    if constexpr (sizeof(R) == 4) {
+        // float32 faces: the fast speeds from p2c's rho h and b^2 of the
+        // same floored states (equal to recomputing them, to rounding)
+        R rhL, b2L, rhR, b2R;
+        r_p2c(P, qL, UL, &rhL, &b2L);
+        r_p2c(P, qR, UR, &rhR, &b2R);
+        r_flux_u(P, n, qL, UL, FL);
+        r_flux_u(P, n, qR, UR, FR);
+        if (!GIVEN) {
+            R lmL, lpL, lmR, lpR;
+            eig_speeds(qL[1 + n], r_fast_speed_from(P, qL[4], rhL, b2L), lmL, lpL);
+            eig_speeds(qR[1 + n], r_fast_speed_from(P, qR[4], rhR, b2R), lmR, lpR);
+            sL = rmin(lmL, lmR);
+            sR = rmax(lpL, lpR);
+        }
+    } else {
+        r_p2c(P, qL, UL);
+        r_p2c(P, qR, UR);
+        r_flux_u(P, n, qL, UL, FL);
+        r_flux_u(P, n, qR, UR, FR);
+        if (!GIVEN) r_speeds(P, n, qL, qR, sL, sR);
+    }
     r_riemann<RIEMANN, MUSCL_OVR>(P, n, qL, qR, UL, UR, FL, FR, sL, sR, F);
 }
 
@@ -682,7 +712,7 @@ AHD void r_c2p_hydro(const Phys<double>& P, double D, double Sx, double Sy, doub
 }
 
 AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
-                       double SB, double S2, double* df);
+                       double SB, double S2, double* df, double tol = 0.0);
 
 AHD double r_f_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
                     double SB, double S2) {
@@ -844,7 +874,7 @@ AHD void r_c2p_start(const Phys<double>& P, const double* U, double* q0, double&
 // b^2 = B^2 / W^2 + (S.B / Z)^2.  Where the reference clamps v^2 or p the
 // clamped quantity is constant and contributes nothing.
 AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
-                       double SB, double S2, double* df) {
+                       double SB, double S2, double* df, double tol) {
     // the reference's divisions regrouped around four quotients (1/Z,
     // 1/(Z+B^2)^2, 1/(1-v^2), Z/(rho W^2)) and one square root: the same
     // residual to rounding, far inside the Newton tolerance
@@ -869,7 +899,8 @@ AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, do
     if (p > P.p_max) { p = P.p_max; pcap = true; }
     const double b2 = B2 * om + vb * vb;
     const double f = (Z - p + 0.5 * B2 + 0.5 * b2 - D) - tau;
-    if (df) {
+    // |f| < tol: the caller stops here, the derivative is not needed
+    if (df && !(fabs(f) < tol)) {
         const bool zfloor = Z < SM;
         const double dA = zfloor ? 0.0 : -2.0 * SB * SB * ZpB * (iZ * iZ * iZ);
         const double dv2 = vcap ? 0.0 : (dA - v2 * 2.0 * ZpB) * iBq;
@@ -896,7 +927,8 @@ AHD bool r_newton_polish(const Phys<double>& P, double& Z, int max_steps, double
     const double tol = 1e-10 * rmax(1.0, tau);
     for (int s = 0;; ++s) {
         double dfdZ = 0.0;
-        const double f = r_f_df_of_Z(P, Z, D, tau, B2, SB, S2, s < max_steps ? &dfdZ : nullptr);
+        const double f =
+            r_f_df_of_Z(P, Z, D, tau, B2, SB, S2, s < max_steps ? &dfdZ : nullptr, tol);
         if (fabs(f) < tol) {
             *steps = s;
             return true;
