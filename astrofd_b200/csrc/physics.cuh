@@ -207,18 +207,19 @@ template <typename R> AHD R hlle_scalar(R qL, R qR, R fL, R fR, R sL, R sR) {
     return (sR * fL - sL * fR + sL * sR * (qR - qL)) / (sR - sL + C<R>::small);
 }
 
-template <int N, typename R>
+// HLLE flux of components [V0, N)
+template <int N, typename R, int V0 = 0>
 AHD void hlle(const R* UL, const R* UR, const R* FL, const R* FR, R sL, R sR, R* out) {
-    if (sL >= R(0)) { for (int v = 0; v < N; ++v) out[v] = FL[v]; return; }
-    if (sR <= R(0)) { for (int v = 0; v < N; ++v) out[v] = FR[v]; return; }
+    if (sL >= R(0)) { for (int v = V0; v < N; ++v) out[v] = FL[v]; return; }
+    if (sR <= R(0)) { for (int v = V0; v < N; ++v) out[v] = FR[v]; return; }
     R inv = sR - sL + C<R>::small;
     if constexpr (sizeof(R) == 4) {
         const R ri = rcp_(inv);
 #pragma unroll
-        for (int v = 0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) * ri;
+        for (int v = V0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) * ri;
     } else {
 #pragma unroll
-        for (int v = 0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) / inv;
+        for (int v = V0; v < N; ++v) out[v] = (sR * FL[v] - sL * FR[v] + sL * sR * (UR[v] - UL[v])) / inv;
     }
 }
 
@@ -387,7 +388,7 @@ AHD void s_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR, int n
 // same (floored) state on the float32 faces
 template <typename R>
 AHD void r_p2c(const Phys<R>& P, const R* qin, R* U, R* rhoh_out = nullptr,
-               R* b2_out = nullptr) {
+               R* b2_out = nullptr, R* B2_out = nullptr, R* vb_out = nullptr) {
     const R gamma = P.gamma;
     R rho = qin[0], vx = qin[1], vy = qin[2], vz = qin[3], p = qin[4];
     R Bx = qin[5], By = qin[6], Bz = qin[7];
@@ -428,21 +429,29 @@ AHD void r_p2c(const Phys<R>& P, const R* qin, R* U, R* rhoh_out = nullptr,
     U[5] = Bx; U[6] = By; U[7] = Bz; U[8] = qin[8];
     if (rhoh_out) *rhoh_out = rhoh;
     if (b2_out) *b2_out = b2;
+    if (B2_out) *B2_out = B2;
+    if (vb_out) *vb_out = vb;
 }
 
 // physical flux from primitives q and U = p2c(q) (flux_rmhd_x/y/z,
 // rmhd_core.py:344-395, recompute p2c internally; reused here)
-template <typename R> AHD void r_flux_u(const Phys<R>& P, int n, const R* q, const R* U, R* F) {
+// B2, Bv: B^2 and B . v of q when the caller has them (p2c of the same q)
+template <typename R>
+AHD void r_flux_u(const Phys<R>& P, int n, const R* q, const R* U, R* F, R B2 = R(-1),
+                  R Bv = R(0)) {
     R v[3] = {q[1], q[2], q[3]}, B[3] = {q[5], q[6], q[7]};
     R p = q[4], psi = q[8];
-    R B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+    if (B2 < R(0)) {
+        B2 = B[0] * B[0] + B[1] * B[1] + B[2] * B[2];
+        Bv = B[0] * v[0] + B[1] * v[1] + B[2] * v[2];
+    }
     R pt = p + R(0.5) * B2;
     R vn = v[n], Bn = B[n];
     F[0] = U[0] * vn;
 #pragma unroll
     for (int m = 0; m < 3; ++m)
         F[1 + m] = (m == n) ? U[1 + m] * vn + pt - Bn * Bn : U[1 + m] * vn - Bn * B[m];
-    F[4] = (U[4] + pt) * vn - (Bn * (B[0] * v[0] + B[1] * v[1] + B[2] * v[2]));
+    F[4] = (U[4] + pt) * vn - (Bn * Bv);
 #pragma unroll
     for (int m = 0; m < 3; ++m) F[5 + m] = (m == n) ? psi : v[m] * Bn - vn * B[m];
     F[8] = P.glm_ch * P.glm_ch * Bn;
@@ -590,11 +599,10 @@ AHD void r_riemann(const Phys<R>& P, int n, const R* qL, const R* qR, const R* U
     if (RIEMANN == ASTRO_RIEMANN_HLLD_FULL) {
         r_hlld_full(P, n, UL, UR, FL, FR, sL, sR, pL, pR, vL, vR, out);
     } else if (RIEMANN == ASTRO_RIEMANN_HLLD) {
-        hlle<9>(UL, UR, FL, FR, sL, sR, out);
-        R h5[5];
-        hllc5(n, UL, UR, FL, FR, sL, sR, pL, pR, vL, vR, h5);
-#pragma unroll
-        for (int v = 0; v < 5; ++v) out[v] = h5[v];
+        // HLLE for the field and psi, HLLC for the hydro block (which the
+        // reference computes with HLLE first and then overwrites)
+        hlle<9, R, 5>(UL, UR, FL, FR, sL, sR, out);
+        hllc5(n, UL, UR, FL, FR, sL, sR, pL, pR, vL, vR, out);
         if (MUSCL_OVR) {
             R sM = contact_speed(n, UL, UR, sL, sR, pL, pR, vL, vR);
             const R* Fm = (sM >= R(0)) ? FL : FR;
@@ -626,11 +634,11 @@ AHD void r_face(const Phys<R>& P, int n, R* qL, R* qR, R* F, R& sL, R& sR) {
     if constexpr (sizeof(R) == 4) {
         // float32 faces: the fast speeds from p2c's rho h and b^2 of the
         // same floored states (equal to recomputing them, to rounding)
-        R rhL, b2L, rhR, b2R;
-        r_p2c(P, qL, UL, &rhL, &b2L);
-        r_p2c(P, qR, UR, &rhR, &b2R);
-        r_flux_u(P, n, qL, UL, FL);
-        r_flux_u(P, n, qR, UR, FR);
+        R rhL, b2L, rhR, b2R, BBL, BBR, vbL, vbR;
+        r_p2c(P, qL, UL, &rhL, &b2L, &BBL, &vbL);
+        r_p2c(P, qR, UR, &rhR, &b2R, &BBR, &vbR);
+        r_flux_u(P, n, qL, UL, FL, BBL, vbL);
+        r_flux_u(P, n, qR, UR, FR, BBR, vbR);
         if (!GIVEN) {
             R lmL, lpL, lmR, lpR;
             eig_speeds(qL[1 + n], r_fast_speed_from(P, qL[4], rhL, b2L), lmL, lpL);
