@@ -632,6 +632,15 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const long cell = tile * mlp::TILE + t;
         const bool valid = cell < a.count;
+        {
+            // the next tile's conserved rows into L2 while this tile runs:
+            // its loads then wait on L2, not DRAM
+            const long nxt = cell + (long)gridDim.x * mlp::TILE;
+            if (nxt < a.count)
+#pragma unroll
+                for (int v = 0; v < 9; ++v)
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + (size_t)v * a.count + nxt));
+        }
         double U[9] = {1, 0, 0, 0, 1, 0, 0, 0, 0};
         if (valid)
 #pragma unroll
