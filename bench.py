@@ -131,25 +131,63 @@ def max_over_ranks(x, world):
 
 # ----------------------------------------------------------------- clocks --
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons during timing."""
+    """SM clock and clock-event (throttle) reasons sampled during timing:
+    every 20 ms through NVML's read-only queries, or every 200 ms from
+    nvidia-smi where NVML is unavailable.  The GPU is addressed by its PCI
+    bus id, which does not depend on CUDA_VISIBLE_DEVICES."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
     def __init__(self, index):
         self.index = index
         self.proc = None
         self.lines = []
+        self.nvml = []
+        self.stop = None
+        self.source = None
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(index)
+            self.bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        except Exception:
+            self.bus = str(index)
 
     def __enter__(self):
         try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(self.bus.encode())
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            self.stop = threading.Event()
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        self.nvml.append((pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM), mx,
+                                          pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.02)
+
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            self.source = "nvml"
+            return self
+        except Exception:
+            self.stop = None
+        try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                ["nvidia-smi", f"--id={self.bus}", f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            self.source = "nvidia-smi"
         except Exception:
             self.proc = None
         return self
@@ -159,6 +197,9 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        if self.stop is not None:
+            self.stop.set()
+            self.t.join(timeout=2)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -167,6 +208,11 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.nvml:
+            sm = [s for s, _, _ in self.nvml]
+            reasons = sorted({k for _, _, r in self.nvml for k, b in self.BITS.items() if r & b})
+            return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(self.nvml[0][1]),
+                    "reasons": reasons, "samples": len(sm), "source": "nvml, 20 ms"}
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
@@ -184,7 +230,7 @@ class ClockSampler:
         if not sm:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx),
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi, 200 ms"}
 
 
 # ------------------------------------------------------------------- GPU ---
