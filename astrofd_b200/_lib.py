@@ -113,6 +113,8 @@ PROTOS = {
     "astro_outflow_yz": (C.c_int, [_DP, C.POINTER(AstroGrid), C.c_int, _VP]),
     "astro_ion_chemistry": (C.c_int, [_DP, C.POINTER(AstroGrid), C.POINTER(AstroChemistry),
                                       C.c_double, _VP]),
+    "astro_step_stage": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP, _DP, _DP,
+                                   C.c_double, C.c_int, C.c_int, _VP, C.c_size_t, _VP, _VP]),
     "astro_diagnostics": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), C.c_int, _DP,
                                     C.c_double, _DP, _VP]),
     "astro_gr_workspace_bytes": (C.c_size_t, [C.POINTER(AstroParams), C.POINTER(AstroGrid),

@@ -159,6 +159,28 @@ class Engine:
                                    rt.ptr(stats), rt.stream_handle(t.device)), "astro_step_gr")
         return out.cpu().numpy() if was_np else out
 
+    def step_stage(self, pr_in, pr_stage, out, dx, dy, dz, dt, rk_order, stage):
+        """Stage `stage` of the SSPRK step from pr_in (astro_step_stage): CUDA
+        tensors only; the stages of one step run in order with no other step
+        on this device in between (the conserved state stays in the cached
+        workspace)."""
+        L = _lib.load()
+        for t in (pr_in, pr_stage, out):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()):
+                raise _lib.AstroError("step_stage takes contiguous CUDA tensors")
+        grid = rt.grid_of(pr_in, dx, dy, dz)
+        nb = L.astro_step_workspace_bytes(C.byref(self.p), C.byref(grid))
+        if nb == 0:
+            _lib.check(-4, "astro_step_stage (configuration)")
+        self._require_network()
+        w = rt.workspace(nb, pr_in.device)
+        stats = self._stats_buffer(pr_in.device)
+        _lib.check(L.astro_step_stage(C.byref(self.p), C.byref(grid), rt.ptr(pr_in),
+                                      rt.ptr(pr_stage), rt.ptr(out), float(dt), int(rk_order),
+                                      int(stage), rt.ptr(w), nb, rt.ptr(stats),
+                                      rt.stream_handle(pr_in.device)), "astro_step_stage")
+        return out
+
     def step_profiled(self, pr, dx, dy, dz, dt, rk_order, out):
         """One step with per-kernel-class CUDA-event times (synchronises)."""
         L = _lib.load()

@@ -77,6 +77,15 @@ def step_ssprk3(pr, dx, dy, dz, dt, out=None):
     return _E.step(pr, dx, dy, dz, dt, 3, out)
 
 
+def step_stage(pr, pr_stage, out, dx, dy, dz, dt, rk_order, stage):
+    """No reference counterpart: stage `stage` of step_ssprk2/3 from the step
+    input pr, this stage's input pr_stage (pr itself at stage 0) into out, for
+    callers that refresh ghost layers between stages (astrofd_b200.slabs).
+    CUDA tensors; the stages of one step run in order, nothing else stepping
+    on the device in between."""
+    return _E.step_stage(pr, pr_stage, out, dx, dy, dz, dt, rk_order, stage)
+
+
 def prim_to_cons(rho, vx, vy, vz, p, gamma=None):
     """Scalars (as the reference) or equal-shaped arrays/tensors."""
     return _pointwise(_E.p2c_array, (rho, vx, vy, vz, p))

@@ -1608,21 +1608,61 @@ size_t astro_step_workspace_bytes(const AstroParams* p, const AstroGrid* g) {
     return layout_of(*p, *g, true).total;
 }
 
-int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, double* pr_out,
-               double dt, int rk_order, void* work, size_t work_bytes, AstroC2PStats* stats,
-               void* stream) {
+// argument checks shared by astro_step and astro_step_stage
+static int step_check(const AstroParams* p, const AstroGrid* g, int rk_order, void* work,
+                      size_t work_bytes) {
     int v = validate(p, g);
     if (v != ASTRO_OK) return v;
-    if (!pr_in || !pr_out || pr_in == pr_out) return ASTRO_E_INVALID;
     if (rk_order != 2 && rk_order != 3) return ASTRO_E_INVALID;
     const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
     if (p->c2p_guess != ASTRO_GUESS_REFERENCE && !learned) return ASTRO_E_INVALID;
     if (learned && (p->physics != ASTRO_RMHD || !p->mlp)) return ASTRO_E_UNSUPPORTED;
+    if (!work || work_bytes < layout_of(*p, *g, true).total) return ASTRO_E_WORKSPACE;
+    return ASTRO_OK;
+}
+
+// One SSPRK stage: faces of cur, update (U_{st-1} -> U_st in the workspace),
+// con2prim into dst.  prf_ready: the float32 copy of cur is already in the
+// workspace; dstf: where the con2prim also writes dst's float32 copy.
+static int run_stage(const AstroParams* p, const AstroGrid* g, const Layout& L, char* w,
+                     const double* pr_in, const double* cur, double* dst, double dt, int nst,
+                     int st, bool prf_ready, float* dstf, AstroC2PStats* stats, cudaStream_t s) {
+    const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
+    const Bounds b = bounds_of(*p, *g);
+    cudaError_t e = face_passes(*p, *g, b, cur, w, L, s, prf_ready);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    UpdArgs u = update_args(*p, *g, b, w, L);
+    u.pr0 = pr_in; u.prk = cur; u.U = (double*)(w + L.U); u.dst = dst;
+    u.dstf = learned ? nullptr : dstf;
+    u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
+    u.defer_c2p = learned ? 1 : 0;
+    e = launch_update(u, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    if (learned) {
+        C2PArgs c;
+        c.U = (const double*)(w + L.U); c.q = dst;
+        c.count = (long)g->nx * g->ny * g->nz;
+        c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
+        c.status = nullptr; c.max_polish = 2;
+        c.fb_count = (unsigned*)(w + L.c2pfb);
+        c.fb_list = (unsigned*)(w + L.c2pfb + 256);
+        c.fb_cap = (unsigned)c2p_fb_capacity(*g);
+        c.qf = dstf;
+        e = launch_c2p_learned(c, s);
+        if (e != cudaSuccess) return ASTRO_E_CUDA;
+    }
+    return ASTRO_OK;
+}
+
+int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, double* pr_out,
+               double dt, int rk_order, void* work, size_t work_bytes, AstroC2PStats* stats,
+               void* stream) {
+    int v = step_check(p, g, rk_order, work, work_bytes);
+    if (v != ASTRO_OK) return v;
+    if (!pr_in || !pr_out || pr_in == pr_out) return ASTRO_E_INVALID;
     const Layout L = layout_of(*p, *g, true);
-    if (!work || work_bytes < L.total) return ASTRO_E_WORKSPACE;
     cudaStream_t s = (cudaStream_t)stream;
     char* w = (char*)work;
-    const Bounds b = bounds_of(*p, *g);
     const int nst = rk_order;
     const double* cur = pr_in;
     double* bufs[2] = {(double*)(w + L.prA), (double*)(w + L.prB)};
@@ -1630,33 +1670,29 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
     for (int st = 0; st < nst; ++st) {
         // stage 0 converts its input to the float32 copy; later stages get the
         // copy from the kernel that produced their primitives
-        cudaError_t e = face_passes(*p, *g, b, cur, w, L, s, st > 0);
-        if (e != cudaSuccess) return ASTRO_E_CUDA;
         double* dst = (st == nst - 1) ? pr_out : bufs[st % 2];
         float* dstf = (mixed && st < nst - 1) ? (float*)(w + L.prf) : nullptr;
-        UpdArgs u = update_args(*p, *g, b, w, L);
-        u.pr0 = pr_in; u.prk = cur; u.U = (double*)(w + L.U); u.dst = dst;
-        u.dstf = learned ? nullptr : dstf;
-        u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
-        u.defer_c2p = learned ? 1 : 0;
-        e = launch_update(u, s);
-        if (e != cudaSuccess) return ASTRO_E_CUDA;
-        if (learned) {
-            C2PArgs c;
-            c.U = (const double*)(w + L.U); c.q = dst;
-            c.count = (long)g->nx * g->ny * g->nz;
-            c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
-            c.status = nullptr; c.max_polish = 2;
-            c.fb_count = (unsigned*)(w + L.c2pfb);
-            c.fb_list = (unsigned*)(w + L.c2pfb + 256);
-            c.fb_cap = (unsigned)c2p_fb_capacity(*g);
-            c.qf = dstf;
-            e = launch_c2p_learned(c, s);
-            if (e != cudaSuccess) return ASTRO_E_CUDA;
-        }
+        v = run_stage(p, g, L, w, pr_in, cur, dst, dt, nst, st, st > 0, dstf, stats, s);
+        if (v != ASTRO_OK) return v;
         cur = dst;
     }
     return ASTRO_OK;
+}
+
+int astro_step_stage(const AstroParams* p, const AstroGrid* g, const double* pr_in,
+                     const double* pr_stage, double* pr_out, double dt, int rk_order, int stage,
+                     void* work, size_t work_bytes, AstroC2PStats* stats, void* stream) {
+    int v = step_check(p, g, rk_order, work, work_bytes);
+    if (v != ASTRO_OK) return v;
+    if (stage < 0 || stage >= rk_order) return ASTRO_E_INVALID;
+    if (!pr_in || !pr_stage || !pr_out || pr_out == pr_in || pr_out == pr_stage)
+        return ASTRO_E_INVALID;
+    if (stage == 0 && pr_stage != pr_in) return ASTRO_E_INVALID;
+    const Layout L = layout_of(*p, *g, true);
+    // the caller may have changed pr_stage's ghosts since it was written: the
+    // float32 copy is made from it here
+    return run_stage(p, g, L, (char*)work, pr_in, pr_stage, pr_out, dt, rk_order, stage, false,
+                     nullptr, stats, (cudaStream_t)stream);
 }
 
 unsigned long long astro_launch_count(void) { return g_launches.load(); }

@@ -15,7 +15,9 @@ The driver exchanges once per step, before the boundary fills
 (solvers/srhd3d_mpi_muscl.py:286-292): the ranks' later RK stages read ghost
 values of the previous step, so a multi-rank run differs from a one-block
 run near the slab faces, as the reference's does.  Only the first rank
-applies the nozzle and only the last the +x outflow.
+applies the nozzle and only the last the +x outflow.  ``step_stagewise``
+also exchanges the output of every RK stage but the last before the next
+stage reads it; the ranks then compute exactly what one block would.
 """
 import torch
 
@@ -65,6 +67,20 @@ class SlabDomain:
             self._bufs = (key, [torch.empty(shape, dtype=pr.dtype, device=pr.device)
                                 for _ in range(4)])
         return self._bufs[1]
+
+    def step_stagewise(self, stage_fn, pr, out, bufs, rk_order):
+        """One SSPRK step with a halo exchange after every stage but the last:
+        stage_fn(pr, pr_stage, dst, stage) runs one stage (e.g. the drop-in
+        cores' step_stage); bufs: two blocks like pr for the intermediate
+        stages.  Returns out."""
+        cur = pr
+        for st in range(rk_order):
+            dst = out if st == rk_order - 1 else bufs[st % 2]
+            stage_fn(pr, cur, dst, st)
+            if st < rk_order - 1:
+                self.exchange(dst)
+            cur = dst
+        return out
 
     def exchange(self, pr):
         """Fill the x ghost layers of ``pr`` (in place) from the neighbours."""

@@ -59,6 +59,10 @@ def parse():
     ap.add_argument("--decomp", default="slab", choices=["slab", "replicas"],
                     help="with --gpus N > 1: x-slabs of one jet with a ghost exchange per "
                          "step, or N independent blocks")
+    ap.add_argument("--halo", default="step", choices=["step", "stage"],
+                    help="with --decomp slab: exchange the ghost layers once per step (the "
+                         "reference driver) or after every RK stage as well (the ranks then "
+                         "compute exactly what one block would)")
     ap.add_argument("--no-graph", action="store_true",
                     help="launch every kernel of the timed steps from the host instead of "
                          "replaying CUDA graphs of one driver iteration")
@@ -237,7 +241,7 @@ class ClockSampler:
 class DriverStep:
     """One reference driver-loop iteration on device tensors."""
 
-    def __init__(self, n, ng, core_cfg, nozzle_cfg, src_cfg, slab=None):
+    def __init__(self, n, ng, core_cfg, nozzle_cfg, src_cfg, slab=None, halo="step"):
         from astrofd_b200.core import boundary, nozzle, rmhd_core, source_terms
         self.B, self.N, self.R, self.S = boundary, nozzle, rmhd_core, source_terms
         self.n, self.ng = n, ng
@@ -245,6 +249,8 @@ class DriverStep:
         self.dt = core_cfg["CFL"] * self.d
         self.noz, self.src = nozzle_cfg, src_cfg
         self.slab = slab
+        self.halo = halo
+        self.bufs = None
         self.rng = np.random.default_rng(1234 + (777 * slab.rank if slab else 0))
 
     def bcs(self, pr):
@@ -267,6 +273,12 @@ class DriverStep:
         if profile:
             _, times, launches = self.R.engine().step_profiled(pr, d, d, d, self.dt, 3, out)
             times = (times, launches)
+        elif self.slab is not None and self.halo == "stage":
+            if self.bufs is None:
+                self.bufs = [out.new_empty(out.shape) for _ in range(2)]
+            self.slab.step_stagewise(
+                lambda p0, pk, dst, st: self.R.step_stage(p0, pk, dst, d, d, d, self.dt, 3, st),
+                pr, out, self.bufs, 3)
         else:
             self.R.step_ssprk3(pr, d, d, d, self.dt, out=out)
         self.bcs(out)
@@ -286,7 +298,7 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     if learned:
         from astrofd_b200 import learned_c2p
         rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
-    step = DriverStep(args.n, 3, core, noz, src, slab_domain(args, world))
+    step = DriverStep(args.n, 3, core, noz, src, slab_domain(args, world), args.halo)
     a = torch.from_numpy(pr_host).to("cuda")
     b = torch.empty_like(a)
     for _ in range(args.warmup):
@@ -367,7 +379,7 @@ def time_e2e(args, world, prec, pr_host, cfgs, learned=False):
     if learned:
         from astrofd_b200 import learned_c2p
         rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
-    step = DriverStep(args.n, 3, core, noz, src, slab_domain(args, world))
+    step = DriverStep(args.n, 3, core, noz, src, slab_domain(args, world), args.halo)
     host_in = torch.from_numpy(pr_host).pin_memory()
     host_out = [torch.empty_like(host_in).pin_memory() for _ in range(2)]
     dev_in = [torch.empty(host_in.shape, dtype=torch.float64, device="cuda") for _ in range(2)]
@@ -755,8 +767,8 @@ def main():
                    "flux_mode": args.flux_mode, "boundaries": args.boundaries,
                    "l2": "inputs larger than L2 (1.6 GB arrays)",
                    "parallelism": ("single GPU" if world == 1 else
-                                   f"x-slabs x{world}, 3 ghost layers exchanged per step "
-                                   "(NCCL send/recv)" if args.decomp == "slab" else
+                                   f"x-slabs x{world}, 3 ghost layers exchanged per "
+                                   f"{args.halo} (NCCL send/recv)" if args.decomp == "slab" else
                                    f"replicas x{world}")},
         "gpu_launches": mixed["launches"],
         "launch_mode": mixed["launch_mode"],

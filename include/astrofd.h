@@ -158,6 +158,19 @@ size_t astro_step_workspace_bytes(const AstroParams* p, const AstroGrid* g);
 int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in,
                double* pr_out, double dt, int rk_order, void* work, size_t work_bytes,
                AstroC2PStats* stats, void* stream);
+/* No reference counterpart: stage `stage` (0 .. rk_order-1) of the same
+ * SSPRK step, for callers that refresh ghost layers between stages (an
+ * x-slab halo exchange per stage makes a multi-rank run equal to the
+ * one-block run; the reference's driver exchanges once per step).  pr_in:
+ * the step's input; pr_stage: this stage's input (pr_in itself at stage 0,
+ * else the previous stage's pr_out, ghosts possibly refreshed); pr_out
+ * distinct from both.  The conserved state between stages lives in `work`
+ * (astro_step_workspace_bytes): the stages of one step run in order on the
+ * same workspace, with no other call on it in between.  Chained, the stages
+ * give astro_step's result exactly. */
+int astro_step_stage(const AstroParams* p, const AstroGrid* g, const double* pr_in,
+                     const double* pr_stage, double* pr_out, double dt, int rk_order, int stage,
+                     void* work, size_t work_bytes, AstroC2PStats* stats, void* stream);
 
 /* Per-kernel-class device time of one step, from CUDA events recorded after
  * every launch.  Classes: 0 face-flux passes, 1 stage update (divergence, RK,

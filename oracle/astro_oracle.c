@@ -1142,6 +1142,31 @@ int oracle_step(const OParams* pa, const double* pr, int nv, int nx, int ny, int
     return step_impl(pa, NULL, pr, nv, nx, ny, nz, dx, dy, dz, dt, rk, out);
 }
 
+static void block_p2c(const OParams* pa, const double* pr, size_t nc, double* U0);
+static void stage_impl(const OParams* pa, const OGR* gr, const double* pr, const double* U0,
+                       const double* cur, double* Uk, double* rhs, int nv, int nx, int ny,
+                       int nz, double dx, double dy, double dz, double dt, int nst, int s,
+                       double* dst);
+
+/* Stage `stage` of an SSPRK step from pr (the step input), prk (this stage's
+ * input), Uk (nm x nc: the previous stage's conserved state in, this stage's
+ * out; ignored in at stage 0): what the stage loop of oracle_step does, for
+ * callers that refresh ghosts between stages. */
+int oracle_stage(const OParams* pa, const double* pr, const double* prk, double* Uk, int nv,
+                 int nx, int ny, int nz, double dx, double dy, double dz, double dt, int rk,
+                 int stage, double* out) {
+    const int nm = pa->physics == 0 ? 5 : 9;
+    const size_t nc = (size_t)nx * ny * nz;
+    double* U0 = malloc(sizeof(double) * nm * nc);
+    double* rhs = malloc(sizeof(double) * (nm + pa->n_passive) * nc);
+    if (!U0 || !rhs) return -1;
+    block_p2c(pa, pr, nc, U0);
+    stage_impl(pa, NULL, pr, U0, prk, Uk, rhs, nv, nx, ny, nz, dx, dy, dz, dt,
+               rk == 3 ? 3 : 2, stage, out);
+    free(U0); free(rhs);
+    return 0;
+}
+
 /* The GR wrappers' steps (grhd_core.py:76-166, grmhd_core.py:80-183): the
  * core step with the GR right-hand side. */
 int oracle_step_gr(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
@@ -1149,32 +1174,30 @@ int oracle_step_gr(const OParams* pa, const OGR* gr, const double* pr, int nv, i
     return step_impl(pa, gr, pr, nv, nx, ny, nz, dx, dy, dz, dt, rk, out);
 }
 
-static int step_impl(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
-                     int nz, double dx, double dy, double dz, double dt, int rk, double* out) {
+/* U0 = prim_to_cons(pr) over the block (the steps' U0 loops) */
+static void block_p2c(const OParams* pa, const double* pr, size_t nc, double* U0) {
     const int nm = pa->physics == 0 ? 5 : 9;
-    const int np = pa->n_passive, po = pa->passive_offset;
-    const size_t nc = (size_t)nx * ny * nz;
-    const int nr = nm + np;
-    double* U0 = malloc(sizeof(double) * nm * nc);
-    double* Uk = malloc(sizeof(double) * nm * nc);
-    double* rhs = malloc(sizeof(double) * nr * nc);
-    double* prA = calloc((size_t)nv * nc, sizeof(double));
-    double* prB = calloc((size_t)nv * nc, sizeof(double));
-    if (!U0 || !Uk || !rhs || !prA || !prB) return -1;
     for (size_t c = 0; c < nc; ++c) {
         double a[9], b[9];
         for (int v = 0; v < nm; ++v) a[v] = pr[v * nc + c];
         if (pa->physics == 0) s_p2c(a, b); else r_p2c(pa, a, b);
         for (int v = 0; v < nm; ++v) U0[v * nc + c] = b[v];
     }
-    const double* cur = pr;
-    const double* prev = NULL;   /* primitives of the previous stage */
-    const int nst = (rk == 3) ? 3 : 2;
-    double* bufs[2] = {prA, prB};
-    for (int s = 0; s < nst; ++s) {
+}
+
+/* Stage s of nst (srhd_core.py:1286-1400, rmhd_core.py:1559-1677): the
+ * right-hand side of cur, Uk <- the stage's SSPRK combination with U0, dst <-
+ * con2prim(Uk), the carried and passive fields; rhs is scratch. */
+static void stage_impl(const OParams* pa, const OGR* gr, const double* pr, const double* U0,
+                       const double* cur, double* Uk, double* rhs, int nv, int nx, int ny,
+                       int nz, double dx, double dy, double dz, double dt, int nst, int s,
+                       double* dst) {
+    const int nm = pa->physics == 0 ? 5 : 9;
+    const int np = pa->n_passive, po = pa->passive_offset;
+    const size_t nc = (size_t)nx * ny * nz;
+    {
         if (gr) oracle_rhs_gr(pa, gr, cur, nv, nx, ny, nz, dx, dy, dz, rhs);
         else oracle_rhs(pa, cur, nv, nx, ny, nz, dx, dy, dz, rhs);
-        double* dst = (s == nst - 1) ? out : bufs[s % 2];
         memset(dst, 0, sizeof(double) * (size_t)nv * nc);
 #pragma omp parallel for schedule(static)
         for (long cl = 0; cl < (long)nc; ++cl) {
@@ -1201,6 +1224,28 @@ static int step_impl(const OParams* pa, const OGR* gr, const double* pr, int nv,
                 else dst[o] = (1.0 / 3.0) * t0 + (2.0 / 3.0) * (cur[o] + dt * r);
             }
         }
+    }
+}
+
+static int step_impl(const OParams* pa, const OGR* gr, const double* pr, int nv, int nx, int ny,
+                     int nz, double dx, double dy, double dz, double dt, int rk, double* out) {
+    const int nm = pa->physics == 0 ? 5 : 9;
+    const size_t nc = (size_t)nx * ny * nz;
+    const int nr = nm + pa->n_passive;
+    double* U0 = malloc(sizeof(double) * nm * nc);
+    double* Uk = malloc(sizeof(double) * nm * nc);
+    double* rhs = malloc(sizeof(double) * nr * nc);
+    double* prA = calloc((size_t)nv * nc, sizeof(double));
+    double* prB = calloc((size_t)nv * nc, sizeof(double));
+    if (!U0 || !Uk || !rhs || !prA || !prB) return -1;
+    block_p2c(pa, pr, nc, U0);
+    const double* cur = pr;
+    const double* prev = NULL;   /* primitives of the previous stage */
+    const int nst = (rk == 3) ? 3 : 2;
+    double* bufs[2] = {prA, prB};
+    for (int s = 0; s < nst; ++s) {
+        double* dst = (s == nst - 1) ? out : bufs[s % 2];
+        stage_impl(pa, gr, pr, U0, cur, Uk, rhs, nv, nx, ny, nz, dx, dy, dz, dt, nst, s, dst);
         prev = cur;
         cur = dst;
     }

@@ -87,6 +87,9 @@ def lib():
         L.oracle_step_gr.argtypes = [C.POINTER(OParams), C.POINTER(OGR), dp, C.c_int, C.c_int,
                                      C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                      C.c_double, C.c_int, dp]
+        L.oracle_stage.argtypes = [C.POINTER(OParams), dp, dp, dp, C.c_int, C.c_int, C.c_int,
+                                   C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                   C.c_int, C.c_int, dp]
         L.oracle_p2c.argtypes = [C.POINTER(OParams), dp, dp, C.c_long]
         L.oracle_c2p.argtypes = [C.POINTER(OParams), dp, dp, C.c_long]
         L.oracle_c2p_counters.argtypes = [C.POINTER(C.c_long), C.c_int]
@@ -159,6 +162,20 @@ def step(params, pr, dx, dy, dz, dt, rk):
     rc = lib().oracle_step(C.byref(params), _dp(pr), *pr.shape, dx, dy, dz, dt, rk, _dp(out))
     if rc != 0:
         raise RuntimeError(f"oracle_step failed ({rc})")
+    return out
+
+
+def stage(params, pr, prk, Uk, dx, dy, dz, dt, rk, st):
+    """Stage st of the SSPRK step from pr; Uk (nm x cells, float64) carries the
+    conserved state between the calls of one step (updated in place)."""
+    pr = np.ascontiguousarray(pr, dtype=np.float64)
+    prk = np.ascontiguousarray(prk, dtype=np.float64)
+    assert Uk.flags.c_contiguous and Uk.dtype == np.float64
+    out = np.zeros_like(pr)
+    rc = lib().oracle_stage(C.byref(params), _dp(pr), _dp(prk), _dp(Uk), *pr.shape, dx, dy, dz,
+                            dt, rk, st, _dp(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_stage failed ({rc})")
     return out
 
 

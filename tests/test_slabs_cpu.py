@@ -145,3 +145,103 @@ def test_driver_loop_on_gloo_ranks_matches_emulation(size, nx, tmp_path):
         got = np.load(tmp_path / f"rank{r}.npy")
         assert np.isfinite(got).all()
         assert np.array_equal(got, want[r]), r
+
+
+# ---- per-stage exchange: the ranks compute exactly what one block would ----
+
+def stage_case(phys):
+    """(G, params, rk, dt, d, ng): a seeded block whose right-hand-side bounds
+    cover its whole interior (PPM with NG = 3; RMHD MUSCL with NG = 2), ghosts
+    filled once as the driver does before a step."""
+    import states
+    if phys == "srhd":
+        ng, rk = 3, 3
+        cfg = dict(GAMMA=5 / 3, P_MAX=2.0, V_MAX=0.9999, RECON="ppm", LIMITER="mc",
+                   RIEMANN="hllc", N_PASSIVE=0, PASSIVE_OFFSET=5)
+    else:
+        ng, rk = 2, 2
+        cfg = dict(GAMMA=4 / 3, P_MAX=2.0, V_MAX=0.9999, GLM_CH=1.0, GLM_CP=0.1, RECON="muscl",
+                   LIMITER="mc", RIEMANN="hlle", N_PASSIVE=0, PASSIVE_OFFSET=9)
+    pr = states.make_state(31 if phys == "srhd" else 32, 8, ng, phys, 0, noise=0.2, bamp=0.1,
+                           vjet=0.6)
+    G = np.concatenate([pr, pr[:, ng:-ng][:, ::-1]], axis=1)[:, :14 + 2 * ng].copy()
+    O.apply_periodic_yz(G, ng)
+    O.apply_outflow_right_x(G, ng)
+    P = O.params_from_config(phys, cfg)
+    d = 1.0 / 8
+    return G, P, rk, 0.1 * d, d, ng
+
+
+@pytest.mark.parametrize("phys", ["srhd", "rmhd"])
+def test_oracle_stages_chain_to_the_step(phys):
+    G, P, rk, dt, d, ng = stage_case(phys)
+    nm = 5 if phys == "srhd" else 9
+    Uk = np.zeros((nm,) + G.shape[1:])
+    cur = G
+    for st in range(rk):
+        cur = O.stage(P, G, cur, Uk, d, d, d, dt, rk, st)
+    assert np.array_equal(cur, O.step(P, G, d, d, d, dt, rk))
+
+
+CHILD_STAGES = r"""
+import sys
+for p in ({root!r}, {oracle!r}, {tests!r}, {golden!r}):
+    sys.path.insert(0, p)
+import numpy as np, torch, torch.distributed as dist
+import oracle as O
+import test_slabs_cpu as T
+from astrofd_b200.slabs import SlabDomain
+dist.init_process_group("gloo", init_method="env://")
+rank = dist.get_rank()
+G, P, rk, dt, d, ng = T.stage_case({phys!r})
+dom = SlabDomain(G.shape[1] - 2 * ng, ng)
+lo, hi = dom.offset, dom.offset + dom.nx + 2 * ng
+pr = torch.from_numpy(G[:, lo:hi].copy())
+Uk = np.zeros(({nm},) + tuple(pr.shape[1:]))
+
+def stage_fn(p0, pk, dst, st):
+    dst.copy_(torch.from_numpy(O.stage(P, p0.numpy(), pk.numpy(), Uk, d, d, d, dt, rk, st)))
+
+out = torch.empty_like(pr)
+dom.step_stagewise(stage_fn, pr, out, [torch.empty_like(pr), torch.empty_like(pr)], rk)
+np.save({out!r} + f"/rank{{rank}}.npy", out.numpy())
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("phys,size", [("srhd", 2), ("srhd", 3), ("rmhd", 2)])
+def test_stagewise_exchange_reproduces_one_block(phys, size, tmp_path):
+    """x-slabs exchanging every RK stage's output give, cell for cell, the
+    one-block step of the same block; exchanging once per step (the
+    reference driver) does not."""
+    G, P, rk, dt, d, ng = stage_case(phys)
+    port = _free_port()
+    code = CHILD_STAGES.format(root=ROOT, oracle=os.path.join(ROOT, "oracle"),
+                               tests=os.path.join(ROOT, "tests"),
+                               golden=os.path.join(ROOT, "tests", "golden"), phys=phys,
+                               nm=5 if phys == "srhd" else 9, out=str(tmp_path))
+    procs = []
+    for r in range(size):
+        env = dict(os.environ, RANK=str(r), WORLD_SIZE=str(size), MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, "-c", code], env=env, text=True,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE))
+    try:
+        for p in procs:
+            _, err = p.communicate(timeout=240)
+            assert p.returncode == 0, err[-3000:]
+    finally:
+        for p in procs:
+            if p.poll() is None:
+                p.kill()
+    ref = O.step(P, G, d, d, d, dt, rk)
+    nx = G.shape[1] - 2 * ng
+    for r in range(size):
+        cnt, off = decompose_x(nx, size, r)[:2]
+        got = np.load(tmp_path / f"rank{r}.npy")
+        assert np.array_equal(got[:, ng:ng + cnt], ref[:, ng + off:ng + off + cnt]), r
+    # without the stage exchanges (a step on the first slab alone) the cells
+    # next to the slab face differ
+    cnt = decompose_x(nx, size, 0)[0]
+    alone = O.step(P, G[:, :cnt + 2 * ng].copy(), d, d, d, dt, rk)
+    assert not np.array_equal(alone[:, ng:ng + cnt], ref[:, ng:ng + cnt])
