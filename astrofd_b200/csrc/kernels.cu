@@ -98,12 +98,10 @@ inline size_t fix_capacity(const AstroGrid& g) {
     return nc / 16 + 1024;
 }
 
-// learned con2prim: cells whose Newton polish fails are listed and solved by
-// a second kernel in dense warps; cells beyond the capacity are solved inline
-inline size_t c2p_fb_capacity(const AstroGrid& g) {
-    const size_t nc = (size_t)g.nx * g.ny * g.nz;
-    return nc / 32 + 1024;
-}
+// learned con2prim: cells whose Newton polish fails are listed (one slot per
+// cell, so the list cannot overflow) and solved by a second kernel in dense
+// warps; the listing kernel then carries no copy of the full solver
+inline size_t c2p_fb_capacity(const AstroGrid& g) { return (size_t)g.nx * g.ny * g.nz; }
 
 Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
     Layout L;
@@ -607,6 +605,9 @@ __device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell) {
 // max_polish Newton steps of the reference's update; cells that do not meet
 // |f| < 1e-10 max(1, tau) then (or whose primitives from Z are invalid) get
 // the reference's complete con2prim, so their result is the reference's.
+// LISTED: a fallback list with a slot for every cell (fb_cap >= count);
+// otherwise every failing cell is solved inline.
+template <bool LISTED>
 __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + mlp::kInferSmem);
@@ -678,15 +679,17 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
             ++n_polish;
             polish_steps += steps;
             done = r_prims_from_Z_checked(P, Z, U, q);
-            if (!done && c2p_defer(a, cell)) continue;
+            if (LISTED && !done && c2p_defer(a, cell)) continue;
         } else {
             ++n_fallback;
             polish_steps += a.max_polish;
             // the reference's complete con2prim, in k_c2p_fallback so that the
             // long solves do not hold up the 31 other cells of this warp
-            if (c2p_defer(a, cell)) continue;
+            if (LISTED && c2p_defer(a, cell)) continue;
         }
-        if (!done) r_c2p<true>(P, U, q, cnt);
+        if constexpr (!LISTED) {
+            if (!done) r_c2p<true>(P, U, q, cnt);
+        }
 #pragma unroll
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
         if (a.qf)
@@ -755,15 +758,17 @@ int sm_count_cached() {
     return g_sm_count;
 }
 
-int g_c2p_blocks_per_sm = 0;
+int g_c2p_blocks_per_sm[2] = {0, 0};
 
-cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
+template <bool LISTED>
+cudaError_t launch_c2p_learned_t(const C2PArgs& a, cudaStream_t s) {
     const long ntiles = (a.count + mlp::TILE - 1) / mlp::TILE;
-    if (!g_c2p_blocks_per_sm) {
+    int& bps = g_c2p_blocks_per_sm[LISTED ? 1 : 0];
+    if (!bps) {
         // prefer the largest shared-memory carveout and size the persistent
         // grid by what is resident per SM: shared memory (one 42 KB tile
         // each), registers, and TMEM (8 blocks x 64 columns)
-        cudaFuncSetAttribute(k_c2p_learned, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(k_c2p_learned<LISTED>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
         int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 65536;
         cudaGetDevice(&dev);
@@ -772,27 +777,36 @@ cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
         cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
         cudaFuncAttributes fa;
         int nb = 4;
-        if (cudaFuncGetAttributes(&fa, k_c2p_learned) == cudaSuccess && smem_sm > 0) {
+        if (cudaFuncGetAttributes(&fa, k_c2p_learned<LISTED>) == cudaSuccess && smem_sm > 0) {
             const int per_block = mlp::kInferSmem + 16 + (int)fa.sharedSizeBytes + reserved;
             const int regs_warp = ((fa.numRegs * 32 + 255) / 256) * 256;
             const int by_smem = smem_sm / per_block;
             const int by_regs = regs_sm / (regs_warp > 0 ? regs_warp * (mlp::TILE / 32) : 1);
             nb = by_smem < by_regs ? by_smem : by_regs;
         }
-        g_c2p_blocks_per_sm = nb < 1 ? 1 : (nb > 8 ? 8 : nb);
+        bps = nb < 1 ? 1 : (nb > 8 ? 8 : nb);
     }
-    const long cap = (long)g_c2p_blocks_per_sm * sm_count_cached();
+    const long cap = (long)bps * sm_count_cached();
     const int grid = (int)(ntiles < cap ? ntiles : cap);
     if (grid <= 0) return cudaSuccess;
     if (a.fb_list && cudaMemsetAsync(a.fb_count, 0, sizeof(unsigned), s) != cudaSuccess)
         return cudaGetLastError();
-    k_c2p_learned<<<grid, mlp::TILE, mlp::kInferSmem + 16, s>>>(a);
+    k_c2p_learned<LISTED><<<grid, mlp::TILE, mlp::kInferSmem + 16, s>>>(a);
     mark(3, s);
-    if (a.fb_list) {
+    if (LISTED) {
         k_c2p_fallback<<<sm_count_cached() * 4, 128, 0, s>>>(a);
         mark(4, s);
     }
     return cudaGetLastError();
+}
+
+// with a fallback list (a slot for every cell) or with inline solves
+cudaError_t launch_c2p_learned(const C2PArgs& a, cudaStream_t s) {
+    if (a.fb_list) {
+        if (a.fb_cap < (unsigned long)a.count) return cudaErrorInvalidValue;
+        return launch_c2p_learned_t<true>(a, s);
+    }
+    return launch_c2p_learned_t<false>(a, s);
 }
 
 // float32 copy of the first nm primitive rows (stage inputs that no
@@ -2018,7 +2032,7 @@ int astro_diagnostics(const AstroParams* p, const AstroGrid* g, int ng, const do
 
 size_t astro_c2p_learned_workspace_bytes(int64_t count) {
     if (count < 0) return 0;
-    return 256 + ((size_t)count / 32 + 1024) * sizeof(unsigned);
+    return 256 + (size_t)count * sizeof(unsigned);
 }
 
 int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
@@ -2037,7 +2051,7 @@ int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, in
         if (count >= (int64_t)UINT32_MAX) return ASTRO_E_SHAPE;
         c.fb_count = (unsigned*)work;
         c.fb_list = (unsigned*)((char*)work + 256);
-        c.fb_cap = (unsigned)((size_t)count / 32 + 1024);
+        c.fb_cap = (unsigned)count;
     }
     return cuda_status(launch_c2p_learned(c, (cudaStream_t)stream));
 }

@@ -260,7 +260,7 @@ int astro_mlp_adam(void* params, float* grad, float* m, float* v, float lr, floa
  * astro_c2p_learned_workspace_bytes(count) bytes they are listed and solved
  * by a second kernel; with work == NULL inline, where one slow state holds up
  * its 128-state tile. */
-size_t astro_c2p_learned_workspace_bytes(int64_t count);
+size_t astro_c2p_learned_workspace_bytes(int64_t count);  /* 256 + 4 count */
 int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
                       int max_polish, void* work, size_t work_bytes, AstroC2PStats* stats,
                       int* status, void* stream);

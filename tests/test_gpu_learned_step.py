@@ -12,8 +12,8 @@ float32 fluxes of the later stages round the slightly different primitives
 differently).
 
 With a random (untrained) network nearly every cell misses the two polish
-steps; those cells go to the fallback list, which overflows its capacity
-(nc/32 + 1024 entries) here, so both the listed and the inline solves run.
+steps; those cells go to the fallback list (a slot for every cell) and are
+all solved by the fallback kernel.
 """
 import numpy as np
 import pytest
@@ -65,14 +65,13 @@ def test_learned_guess_matches_reference_guess(precision):
     assert st["learned_polish"] > 0.98 * st["cells"], st
 
 
-def test_fallback_list_and_inline_solves():
+def test_fallback_list_solves():
     ref, _ = _run("fp64", "reference", None)
     # an untrained network whose outputs start ~e^5 too large
     got, st = _run("fp64", "learned", LC.init_params(seed=11, ymu=np.array([5.0, 5.0])))
     nc = (N + 2 * NG) ** 3
-    cap = nc // 32 + 1024
-    # more cells fell back per launch than the list holds: both paths ran
-    assert st["learned_fallback"] > 3 * STEPS * cap, st
+    # most cells fell back and were listed
+    assert st["learned_fallback"] > 0.5 * 3 * STEPS * nc, st
     assert np.isfinite(got).all()
     err = PT.normwise(got, ref)
     assert err < TOL["fp64"], err

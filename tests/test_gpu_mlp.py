@@ -166,8 +166,8 @@ def test_training_on_jet_states_gains():
 
 def test_listed_and_inline_fallback_agree():
     """The states whose polish fails are solved by the reference's complete
-    con2prim either way: listed for a second kernel (with a workspace; beyond
-    its capacity inline) or all inline.  The same source inlined into two
+    con2prim either way: listed for a second kernel (with a workspace, a slot
+    for every state) or inline (without).  The same source inlined into two
     kernels may contract floating-point operations differently, so agreement
     is to the solver's tolerance, on states with one physical root (v.B = 0):
     relative 1e-6 (|f| < 1e-10 max(1, tau) leaves p free to ~1e-5 when
@@ -179,8 +179,8 @@ def test_listed_and_inline_fallback_agree():
     q2, st2 = LC.c2p_learned(e, U, bad, max_polish=2, listed=False)
     assert st1["status"] == 0 and st2["status"] == 0
     n = U.shape[1]
-    # most states fall back, more than the list holds: listed and inline both ran
-    assert st1["learned_fallback"] == st2["learned_fallback"] > n // 32 + 1024
+    # most states fall back
+    assert st1["learned_fallback"] == st2["learned_fallback"] > n // 2
     ref = e.c2p_array(U)
     ok = torch.isfinite(ref).all(0)
     assert ok.float().mean() > 0.99
