@@ -115,6 +115,8 @@ PROTOS = {
                                       C.c_double, _VP]),
     "astro_step_stage": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP, _DP, _DP,
                                    C.c_double, C.c_int, C.c_int, _VP, C.c_size_t, _VP, _VP]),
+    "astro_prof_start": (C.c_int, [C.c_int, _VP]),
+    "astro_prof_stop": (C.c_int, [C.POINTER(AstroKernelTimes)]),
     "astro_diagnostics": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), C.c_int, _DP,
                                     C.c_double, _DP, _VP]),
     "astro_gr_workspace_bytes": (C.c_size_t, [C.POINTER(AstroParams), C.POINTER(AstroGrid),

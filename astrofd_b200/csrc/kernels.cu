@@ -24,6 +24,7 @@
 
 #include <atomic>
 #include <mutex>
+#include <vector>
 
 #include "mlp.cuh"
 #include "physics.cuh"
@@ -35,22 +36,43 @@ namespace {
 // process-wide count of kernels this library has launched (diagnostic only)
 std::atomic<unsigned long long> g_launches{0};
 
-// Optional per-launch CUDA-event timing used by astro_step_profiled: an event
-// is recorded after every launch; the gap to the previous event is charged to
-// the launch's kernel class.
+// Optional per-launch CUDA-event timing (astro_step_profiled, and the
+// astro_prof_start/stop sessions): an event is recorded after every launch;
+// the gap to the previous event is charged to the launch's kernel class.
 struct Prof {
-    static constexpr int kMax = 64;
-    cudaEvent_t ev[kMax + 1];
-    int kind[kMax];
+    std::vector<cudaEvent_t> ev;  // cap + 1
+    std::vector<int> kind;        // cap
     int n = 0;
     bool on = false;
+    int create(int cap) {
+        ev.assign((size_t)cap + 1, nullptr);
+        kind.assign((size_t)cap, 0);
+        for (auto& e : ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return ASTRO_E_CUDA;
+        return ASTRO_OK;
+    }
+    int cap() const { return (int)kind.size(); }
+    void sum(AstroKernelTimes* t) const {
+        memset(t, 0, sizeof(*t));
+        for (int i = 0; i < n; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            const int k = kind[i] < 5 ? kind[i] : 2;
+            t->ms[k] += ms;
+            t->launches[k] += 1;
+        }
+    }
+    ~Prof() {
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
 };
 thread_local Prof* t_prof = nullptr;
 
 inline void mark(int kind, cudaStream_t s) {
     g_launches.fetch_add(1, std::memory_order_relaxed);
     Prof* P = t_prof;
-    if (P && P->on && P->n < Prof::kMax) {
+    if (P && P->on && P->n < P->cap()) {
         cudaEventRecord(P->ev[P->n + 1], s);
         P->kind[P->n++] = kind;
     }
@@ -1715,9 +1737,9 @@ int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* 
                         double* pr_out, double dt, int rk_order, void* work, size_t work_bytes,
                         AstroC2PStats* stats, void* stream, AstroKernelTimes* times) {
     if (!times) return ASTRO_E_INVALID;
+    if (t_prof) return ASTRO_E_INVALID;  // a profiling session is running
     Prof P;
-    for (int i = 0; i <= Prof::kMax; ++i)
-        if (cudaEventCreate(&P.ev[i]) != cudaSuccess) return ASTRO_E_CUDA;
+    if (P.create(64) != ASTRO_OK) return ASTRO_E_CUDA;
     cudaStream_t s = (cudaStream_t)stream;
     cudaEventRecord(P.ev[0], s);
     P.on = true;
@@ -1726,16 +1748,31 @@ int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* 
     t_prof = nullptr;
     if (rc == ASTRO_OK && cudaEventSynchronize(P.ev[P.n]) != cudaSuccess) rc = ASTRO_E_CUDA;
     memset(times, 0, sizeof(*times));
-    if (rc == ASTRO_OK) {
-        for (int i = 0; i < P.n; ++i) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, P.ev[i], P.ev[i + 1]);
-            const int k = P.kind[i] < 5 ? P.kind[i] : 2;
-            times->ms[k] += ms;
-            times->launches[k] += 1;
-        }
+    if (rc == ASTRO_OK) P.sum(times);
+    return rc;
+}
+
+int astro_prof_start(int max_launches, void* stream) {
+    if (max_launches < 1 || max_launches > (1 << 20) || t_prof) return ASTRO_E_INVALID;
+    Prof* P = new Prof();
+    if (P->create(max_launches) != ASTRO_OK) {
+        delete P;
+        return ASTRO_E_CUDA;
     }
-    for (int i = 0; i <= Prof::kMax; ++i) cudaEventDestroy(P.ev[i]);
+    cudaEventRecord(P->ev[0], (cudaStream_t)stream);
+    P->on = true;
+    t_prof = P;
+    return ASTRO_OK;
+}
+
+int astro_prof_stop(AstroKernelTimes* times) {
+    Prof* P = t_prof;
+    if (!P || !times) return ASTRO_E_INVALID;
+    t_prof = nullptr;
+    int rc = cudaEventSynchronize(P->ev[P->n]) == cudaSuccess ? ASTRO_OK : ASTRO_E_CUDA;
+    memset(times, 0, sizeof(*times));
+    if (rc == ASTRO_OK) P->sum(times);
+    delete P;
     return rc;
 }
 

@@ -63,9 +63,9 @@ def parse():
                     help="with --decomp slab: exchange the ghost layers once per step (the "
                          "reference driver) or after every RK stage as well (the ranks then "
                          "compute exactly what one block would)")
-    ap.add_argument("--no-graph", action="store_true",
-                    help="launch every kernel of the timed steps from the host instead of "
-                         "replaying CUDA graphs of one driver iteration")
+    ap.add_argument("--graph", action="store_true",
+                    help="replay CUDA graphs of one driver iteration in the timed steps "
+                         "(kernel-class times then come from profiled steps after them)")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -288,6 +288,7 @@ class DriverStep:
 
 
 def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
+    import ctypes as C
     import torch
     from astrofd_b200 import _lib
     from astrofd_b200.core import rmhd_core
@@ -304,13 +305,12 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     for _ in range(args.warmup):
         a, b, _ = step(a, b)
     L = _lib.load()
-    # one driver iteration is a fixed sequence of kernels on fixed buffers (no
-    # host-drawn nozzle perturbation in this workload): capture a -> b and
-    # b -> a as CUDA graphs and replay them, which removes the launch gaps
-    # between the ~30 kernels of a step.  Slab runs (NCCL exchange in the
-    # step) launch eagerly.
+    # --graph: one driver iteration is a fixed sequence of kernels on fixed
+    # buffers (no host-drawn nozzle perturbation in this workload): capture
+    # a -> b and b -> a as CUDA graphs and replay them.  Slab runs (NCCL
+    # exchange in the step) launch eagerly.
     graphs, per_iter, graph_note = None, 0, "eager launches"
-    if not args.no_graph and step.slab is None:
+    if args.graph and step.slab is None:
         try:
             torch.cuda.synchronize()
             g1, g2 = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
@@ -330,10 +330,18 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     prof_ms = np.zeros(5)
     prof_n = np.zeros(5, dtype=np.int64)
+    # eager timed steps of the profiled arm: an event after every launch
+    # (astro_prof_start/stop), read once after the timed region, so the
+    # kernel-class times are those of the timed steps, with no host
+    # synchronisation among them
+    session = profile and graphs is None
     barrier(world)
     torch.cuda.synchronize()
     l0 = L.astro_launch_count()
     with ClockSampler(torch.cuda.current_device()) as clk:
+        if session:
+            _lib.check(L.astro_prof_start(64 * args.steps + 64, C.c_void_p(stream.cuda_stream)),
+                       "astro_prof_start")
         e0.record(stream)
         for i in range(args.steps):
             if graphs is not None:
@@ -343,25 +351,33 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
                 a, b, _ = step(a, b)
         e1.record(stream)
         torch.cuda.synchronize()
+    if session:
+        kt = _lib.AstroKernelTimes()
+        _lib.check(L.astro_prof_stop(C.byref(kt)), "astro_prof_stop")
+        prof_ms += np.array([kt.ms[i] for i in range(5)])
+        prof_n += np.array([kt.launches[i] for i in range(5)])
     barrier(world)
     launches = (L.astro_launch_count() - l0) if graphs is None else per_iter * args.steps
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     finite = bool(torch.isfinite(a).all().item())
     stats = rmhd_core.c2p_stats(reset=True)
-    state = a.clone() if profile else a
-    # per-kernel-class times from a few more steps after the timed region:
-    # astro_step_profiled synchronises after every step, which would put
-    # host gaps into the timed steps
-    prof_steps = max(1, min(args.steps, 3)) if profile else 0
-    for _ in range(prof_steps):
-        a, b, t = step(a, b, profile=True)
-        prof_ms += np.array(t[0])
-        prof_n += np.array(t[1])
+    state = a
+    prof_steps, times_from = (args.steps, "the timed steps") if session else (0, None)
+    if profile and not session:
+        # graph replay: per-kernel-class times from a few more steps after the
+        # timed ones (astro_step_profiled synchronises after every step)
+        state = a.clone()
+        prof_steps = max(1, min(args.steps, 3))
+        times_from = f"{prof_steps} profiled steps after the timed ones"
+        for _ in range(prof_steps):
+            a, b, t = step(a, b, profile=True)
+            prof_ms += np.array(t[0])
+            prof_n += np.array(t[1])
     if graphs is not None:
         del graphs
     return dict(ms=ms, launches=int(launches), prof_ms=prof_ms, prof_n=prof_n,
                 prof_steps=prof_steps, clocks=clk.summary(), finite=finite, state=state,
-                c2p=stats, launch_mode=graph_note)
+                c2p=stats, launch_mode=graph_note, times_from=times_from)
 
 
 def time_e2e(args, world, prec, pr_host, cfgs, learned=False):
@@ -777,7 +793,7 @@ def main():
         "kernel_ms_per_step": {k: round(mixed["prof_ms"][c] / mixed["prof_steps"], 3)
                                for k, c in (("face", 0), ("update", 1), ("c2p_learned", 3),
                                             ("c2p_fallback", 4), ("other", 2))},
-        "kernel_times_from": f"{mixed['prof_steps']} profiled steps after the timed ones",
+        "kernel_times_from": mixed["times_from"],
         "finite": mixed["finite"],
         "c2p": mixed["c2p"],
     }

@@ -191,6 +191,14 @@ int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* 
 /* Number of kernels this library has launched in the process so far
  * (a diagnostic counter; no counterpart in the reference). */
 unsigned long long astro_launch_count(void);
+/* No reference counterpart: kernel-class times over any sequence of this
+ * library's calls, without host synchronisation in between.
+ * astro_prof_start records an event on `stream`, then one after each of the
+ * library's launches made from the calling thread (all on that stream, up to
+ * max_launches); astro_prof_stop waits for the last event and charges each
+ * gap to its launch's class (classes as in astro_step_profiled). */
+int astro_prof_start(int max_launches, void* stream);
+int astro_prof_stop(AstroKernelTimes* times);
 
 /* --- CFL speed ----------------------------------------------------------
  * Replaces srhd_core.max_char_speed (core/srhd_core.py:1268): writes the max
