@@ -378,13 +378,15 @@ template <typename RF> __device__ __forceinline__ double ldf(const void* p, size
 constexpr int kUpdateBlock = 128;
 
 // DEFER: the learned con2prim runs in its own kernel, so this one only writes
-// U (the con2prim code is compiled out, which frees registers for loads in
-// flight: 6 blocks of 128 threads per SM).  Every load is a plain coalesced
+// U (the con2prim code is compiled out).  Every load is a plain coalesced
 // load with no dependence on an earlier one, so a thread's loads overlap each
-// other; staging them through shared memory with per-thread cp.async streamed
-// more slowly on B200 (4.2 against 6.4 TB/s for the same bytes).
+// other; 8 blocks of 128 threads per SM (64 registers, a few spilled) keep
+// more of them in flight than 6 blocks at 80 registers (3.81 against 3.96
+// ms/step; 10 and 12 blocks spill too much).  Staging the loads through
+// shared memory with per-thread cp.async streamed more slowly on B200 (4.2
+// against 6.4 TB/s for the same bytes).
 template <int PHYS, typename RF, bool DEFER, bool PASSIVE>
-__global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 6) k_update(UpdArgs a) {
+__global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 8) k_update(UpdArgs a) {
     constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
     constexpr int T = kUpdateBlock;
     const unsigned nc32 = (unsigned)a.nx * (unsigned)a.ny * (unsigned)a.nz;
