@@ -83,7 +83,40 @@ CASES = [
        GAMMA=5.0 / 3.0),
 ]
 
+# Non-cubic blocks (the x-slabs of the reference's MPI driver have unequal
+# extents), with dx = 1/nx, dy = 1/ny, dz = 1/nz all different, and blocks one
+# interior cell thick in one direction.
+CASES += [
+    _c("s_muscl_mc_hllc_ragged", "srhd", "muscl", "mc", "hllc", 3, 2, seed=121, n=(5, 9, 7)),
+    _c("s_weno_hlle_ragged", "srhd", "weno", "mc", "hlle", 2, 3, seed=122, n=(9, 4, 6)),
+    _c("s_ppm_hlle_ragged_pass1", "srhd", "ppm", "mc", "hlle", 3, 3, n_extra=1, seed=123,
+       n=(6, 7, 5)),
+    _c("s_muscl_minmod_hlle_thin", "srhd", "muscl", "minmod", "hlle", 2, 2, seed=124,
+       n=(1, 6, 5)),
+    _c("r_weno_hlld_ragged", "rmhd", "weno", "mc", "hlld", 3, 3, seed=221, n=(6, 10, 5)),
+    _c("r_muscl_mc_hlle_ragged_resist", "rmhd", "muscl", "mc", "hlle", 2, 2, seed=222,
+       n=(11, 5, 8), RESISTIVE_ENABLED=True, RESISTIVITY=1e-3),
+    _c("r_ppm_hlld_ragged", "rmhd", "ppm", "mc", "hlld", 2, 3, seed=223, n=(4, 6, 9)),
+    _c("r_weno_hlle_thin", "rmhd", "weno", "mc", "hlle", 3, 3, seed=224, n=(5, 3, 1)),
+]
+
 CASE_BY_NAME = {c["name"]: c for c in CASES}
+
+
+def sizes(c):
+    """Interior cells (nx, ny, nz) of a case."""
+    n = c["n"]
+    return (n, n, n) if isinstance(n, int) else tuple(n)
+
+
+def spacing(c):
+    """(dx, dy, dz) of a case: the unit box over its interior cells."""
+    return tuple(1.0 / m for m in sizes(c))
+
+
+def step_dt(c):
+    """dt of the single-step fixtures."""
+    return DT_FRACTION * min(spacing(c))
 
 
 def _gr(name, physics, recon, limiter, riemann, rk, ng, gr, offs_x, seed, **kw):

@@ -23,7 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 import numpy as np  # noqa: E402
-from cases import CASES, CASE_BY_NAME, DT_FRACTION, GR_CASES, GR_BY_NAME  # noqa: E402
+from cases import CASES, CASE_BY_NAME, DT_FRACTION, GR_CASES, GR_BY_NAME, spacing, step_dt  # noqa: E402
 import states  # noqa: E402
 
 SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
@@ -52,21 +52,21 @@ def run_case(name, ref, out):
     mod.configure(p)
     pr = states.make_state(c["seed"], c["n"], c["ng"], c["physics"],
                            c["n_extra"] + c["pad"], **c["state"])
-    n = pr.shape[1]
-    dx = dy = dz = 1.0 / c["n"]
+    nx, ny, nz = pr.shape[1:]
+    dx, dy, dz = spacing(c)
     if c["physics"] == "srhd":
         rhs_fn = {"muscl": S.compute_rhs_muscl, "ppm": S.compute_rhs_ppm,
                   "weno": S.compute_rhs_weno}[p["RECON"]]
     else:
         rhs_fn = {"muscl": R.compute_rhs_rmhd, "ppm": R.compute_rhs_ppm,
                   "weno": R.compute_rhs_weno}[p["RECON"]]
-    rhs = rhs_fn(pr, n, n, n, dx, dy, dz)
-    dt = DT_FRACTION * dx
+    rhs = rhs_fn(pr, nx, ny, nz, dx, dy, dz)
+    dt = step_dt(c)
     step = mod.step_ssprk3 if c["rk"] == 3 else mod.step_ssprk2
     out_pr = step(pr.copy(), dx, dy, dz, dt)
     extra = {}
     if c["physics"] == "srhd":
-        extra["max_char_speed"] = np.array(S.max_char_speed(pr, n, n, n))
+        extra["max_char_speed"] = np.array(S.max_char_speed(pr, nx, ny, nz))
     np.savez_compressed(out, pr_in=pr, rhs=rhs, step_out=out_pr,
                         dt=np.array(dt), params=json.dumps(p), **extra)
 

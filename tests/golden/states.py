@@ -20,7 +20,8 @@ def make_state(seed, n, ng, physics, n_extra=0, vjet=0.99, noise=0.3,
                bamp=0.3, stripes=True, n_is=0):
     """Return a rough jet-like primitive block.
 
-    n        interior cells per dimension (cube)
+    n        interior cells: an int (a cube) or (nx, ny, nz); a cube draws
+             the same random numbers in the same order either way
     ng       ghost layers
     physics  "srhd" (5 primitives) or "rmhd" (9 primitives)
     n_extra  extra passive variables appended after the base primitives
@@ -29,26 +30,27 @@ def make_state(seed, n, ng, physics, n_extra=0, vjet=0.99, noise=0.3,
              primitives and the passives (SRHD blocks of 15+ variables)
     """
     rng = np.random.default_rng(seed)
-    N = n + 2 * ng
+    nx, ny, nz = (n, n, n) if np.isscalar(n) else n
+    S = (nx + 2 * ng, ny + 2 * ng, nz + 2 * ng)
     nm = n_main(physics)
     nv = nm + n_is + n_extra
-    pr = np.zeros((nv, N, N, N), dtype=np.float64)
+    pr = np.zeros((nv,) + S, dtype=np.float64)
 
     def u(*shape):
         return 2.0 * rng.random(shape) - 1.0
 
-    pr[0] = 1.0 * (1.0 + noise * u(N, N, N))
-    pr[1] = 0.3 * u(N, N, N)
-    pr[2] = 0.3 * u(N, N, N)
-    pr[3] = 0.3 * u(N, N, N)
-    pr[4] = 0.01 * (1.0 + 0.5 * u(N, N, N))
+    pr[0] = 1.0 * (1.0 + noise * u(*S))
+    pr[1] = 0.3 * u(*S)
+    pr[2] = 0.3 * u(*S)
+    pr[3] = 0.3 * u(*S)
+    pr[4] = 0.01 * (1.0 + 0.5 * u(*S))
 
     # relativistic jet core along x through the middle of the y/z plane
-    c = 0.5 * (N - 1)
-    jj, kk = np.meshgrid(np.arange(N), np.arange(N), indexing="ij")
-    r = np.sqrt((jj - c) ** 2 + (kk - c) ** 2)
-    core = r < 0.3 * N
-    for i in range(N):
+    cy, cz = 0.5 * (S[1] - 1), 0.5 * (S[2] - 1)
+    jj, kk = np.meshgrid(np.arange(S[1]), np.arange(S[2]), indexing="ij")
+    r = np.sqrt((jj - cy) ** 2 + (kk - cz) ** 2)
+    core = r < 0.3 * min(S[1], S[2])
+    for i in range(S[0]):
         if stripes and i % 3 == 2:
             continue  # leave some ambient x-planes for strong jumps
         pr[0, i][core] = 0.1 * (1.0 + 0.1 * rng.random(core.sum()))
@@ -62,15 +64,15 @@ def make_state(seed, n, ng, physics, n_extra=0, vjet=0.99, noise=0.3,
     pr[1:4] *= fac
 
     if physics == "rmhd":
-        pr[5] = bamp * u(N, N, N)
-        pr[6] = bamp * u(N, N, N)
-        pr[7] = bamp * u(N, N, N)
-        pr[8] = 0.01 * u(N, N, N)
+        pr[5] = bamp * u(*S)
+        pr[6] = bamp * u(*S)
+        pr[7] = bamp * u(*S)
+        pr[8] = 0.01 * u(*S)
 
     for m in range(n_is):
-        pr[nm + m] = 0.003 * u(N, N, N)
+        pr[nm + m] = 0.003 * u(*S)
     for t in range(n_extra):
-        pr[nm + n_is + t] = rng.random((N, N, N))
+        pr[nm + n_is + t] = rng.random(S)
     return np.ascontiguousarray(pr)
 
 

@@ -14,7 +14,7 @@ import torch
 
 import oracle as O
 import parity as PT
-from cases import CASES
+from cases import CASES, spacing
 
 pytestmark = pytest.mark.gpu
 
@@ -49,9 +49,7 @@ def test_rhs_fp64_vs_reference(case):
     d = PT.load(case["name"])
     m = _mods(case)
     pr = torch.from_numpy(d["pr_in"]).to(DEV)
-    n = pr.shape[1]
-    dx = 1.0 / case["n"]
-    r = _rhs_fn(m, case)(pr, n, n, n, dx, dx, dx).cpu().numpy()
+    r = _rhs_fn(m, case)(pr, *pr.shape[1:], *spacing(case)).cpu().numpy()
     assert r.shape == d["rhs"].shape
     assert PT.normwise(r, d["rhs"]) < 1e-10
 
@@ -61,9 +59,8 @@ def test_step_fp64_vs_reference(case):
     d = PT.load(case["name"])
     m = _mods(case)
     pr = torch.from_numpy(d["pr_in"]).to(DEV)
-    dx = 1.0 / case["n"]
     step = m.step_ssprk3 if case["rk"] == 3 else m.step_ssprk2
-    out = step(pr, dx, dx, dx, float(d["dt"])).cpu().numpy()
+    out = step(pr, *spacing(case), float(d["dt"])).cpu().numpy()
     g = d["step_out"]
     if HLLD_FULL(case):
         msk = PT.sane_mask(g, case["physics"])
@@ -77,9 +74,7 @@ def test_numpy_inputs_round_trip_through_device(case):
     """The drop-in keeps the reference's numpy-in/numpy-out convention."""
     d = PT.load(case["name"])
     m = _mods(case)
-    n = d["pr_in"].shape[1]
-    dx = 1.0 / case["n"]
-    r = _rhs_fn(m, case)(d["pr_in"], n, n, n, dx, dx, dx)
+    r = _rhs_fn(m, case)(d["pr_in"], *d["pr_in"].shape[1:], *spacing(case))
     assert isinstance(r, np.ndarray)
     assert PT.normwise(r, d["rhs"]) < 1e-10
 
@@ -89,9 +84,7 @@ def test_rhs_mixed_precision_close_to_fp64(case):
     d = PT.load(case["name"])
     m = _mods(case, dict(PRECISION="mixed"))
     pr = torch.from_numpy(d["pr_in"]).to(DEV)
-    n = pr.shape[1]
-    dx = 1.0 / case["n"]
-    r = _rhs_fn(m, case)(pr, n, n, n, dx, dx, dx).cpu().numpy()
+    r = _rhs_fn(m, case)(pr, *pr.shape[1:], *spacing(case)).cpu().numpy()
     assert np.all(np.isfinite(r[:5]))
     assert PT.normwise(r, d["rhs"]) < 5e-3
 
@@ -102,8 +95,7 @@ def test_max_char_speed(case):
     d = PT.load(case["name"])
     m = _mods(case)
     pr = torch.from_numpy(d["pr_in"]).to(DEV)
-    n = pr.shape[1]
-    assert m.max_char_speed(pr, n, n, n) == pytest.approx(float(d["max_char_speed"]), rel=1e-14)
+    assert m.max_char_speed(pr, *pr.shape[1:]) == pytest.approx(float(d["max_char_speed"]), rel=1e-14)
 
 
 def test_c2p_p2c_batches():

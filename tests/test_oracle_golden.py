@@ -5,7 +5,7 @@ import pytest
 
 import oracle as O
 import parity as PT
-from cases import CASES
+from cases import CASES, spacing
 
 HLLD_FULL = lambda c: c["params"]["RIEMANN"] == "hlld_full"
 
@@ -19,8 +19,8 @@ def _built():
 def test_rhs_matches_reference(case):
     d = PT.load(case["name"])
     P = O.params_from_config(case["physics"], PT.params_of(d))
-    dx = 1.0 / case["n"]
-    r = O.rhs(P, d["pr_in"], dx, dx, dx)
+    dx, dy, dz = spacing(case)
+    r = O.rhs(P, d["pr_in"], dx, dy, dz)
     assert r.shape == d["rhs"].shape
     # FP64 restatement vs Numba(fastmath): normwise per variable
     assert PT.normwise(r, d["rhs"]) < 1e-10
@@ -30,8 +30,8 @@ def test_rhs_matches_reference(case):
 def test_step_matches_reference(case):
     d = PT.load(case["name"])
     P = O.params_from_config(case["physics"], PT.params_of(d))
-    dx = 1.0 / case["n"]
-    out = O.step(P, d["pr_in"], dx, dx, dx, float(d["dt"]), case["rk"])
+    dx, dy, dz = spacing(case)
+    out = O.step(P, d["pr_in"], dx, dy, dz, float(d["dt"]), case["rk"])
     g = d["step_out"]
     if HLLD_FULL(case):
         # con2prim is ill-conditioned where the reference HLLD blew up
