@@ -226,7 +226,7 @@ class Engine:
     def p2c_array(self, q):
         L = _lib.load()
         t, was_np = rt.to_device(q)
-        t = t.reshape(self.nm, -1).contiguous()
+        t = t.reshape(self.nm, t.numel() // self.nm).contiguous()
         out = torch.empty_like(t)
         _lib.check(L.astro_p2c(C.byref(self.p), rt.ptr(t), rt.ptr(out), t.shape[1],
                                rt.stream_handle(t.device)), "astro_p2c")
@@ -235,7 +235,7 @@ class Engine:
     def c2p_array(self, U):
         L = _lib.load()
         t, was_np = rt.to_device(U)
-        t = t.reshape(self.nm, -1).contiguous()
+        t = t.reshape(self.nm, t.numel() // self.nm).contiguous()
         out = torch.empty_like(t)
         stats = self._stats_buffer(t.device)
         _lib.check(L.astro_c2p(C.byref(self.p), rt.ptr(t), rt.ptr(out), t.shape[1],

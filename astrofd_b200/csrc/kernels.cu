@@ -1848,8 +1848,9 @@ int astro_outflow_yz(double* pr, const AstroGrid* g, int ng, void* stream) {
 }
 
 int astro_p2c(const AstroParams* p, const double* prim, double* cons, int64_t count, void* stream) {
-    if (!p || !prim || !cons || count < 0) return ASTRO_E_INVALID;
-    if (count == 0) return ASTRO_OK;
+    if (!p || count < 0) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;  // an empty batch may pass null arrays
+    if (!prim || !cons) return ASTRO_E_INVALID;
     k_p2c<<<grid_for(count, 128), 128, 0, (cudaStream_t)stream>>>(*p, prim, cons, count);
     mark(2, (cudaStream_t)stream);
     return cuda_status(cudaGetLastError());
@@ -1857,8 +1858,9 @@ int astro_p2c(const AstroParams* p, const double* prim, double* cons, int64_t co
 
 int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t count,
               AstroC2PStats* stats, void* stream) {
-    if (!p || !prim || !cons || count < 0) return ASTRO_E_INVALID;
-    if (count == 0) return ASTRO_OK;
+    if (!p || count < 0) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;  // an empty batch may pass null arrays
+    if (!prim || !cons) return ASTRO_E_INVALID;
     k_c2p<<<grid_for(count, 128), 128, 0, (cudaStream_t)stream>>>(*p, cons, prim, count, stats);
     mark(2, (cudaStream_t)stream);
     return cuda_status(cudaGetLastError());
@@ -2077,9 +2079,10 @@ size_t astro_c2p_learned_workspace_bytes(int64_t count) {
 int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, int64_t count,
                       int max_polish, void* work, size_t work_bytes, AstroC2PStats* stats,
                       int* status, void* stream) {
-    if (!p || !cons || !prim || count < 0 || p->physics != ASTRO_RMHD) return ASTRO_E_INVALID;
+    if (!p || count < 0 || p->physics != ASTRO_RMHD) return ASTRO_E_INVALID;
     if (max_polish < 0 || max_polish > 50) return ASTRO_E_INVALID;
-    if (count == 0) return ASTRO_OK;
+    if (count == 0) return ASTRO_OK;  // an empty batch may pass null arrays
+    if (!cons || !prim) return ASTRO_E_INVALID;
     C2PArgs c;
     c.U = cons; c.q = prim; c.count = count; c.p = *p;
     c.net = (const mlp::Params*)p->mlp; c.stats = stats; c.status = status;
@@ -2096,8 +2099,9 @@ int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, in
 }
 
 int astro_c2p_features(const double* cons, float* x, int64_t count, void* stream) {
-    if (!cons || !x || count < 0) return ASTRO_E_INVALID;
-    if (count == 0) return ASTRO_OK;
+    if (count < 0) return ASTRO_E_INVALID;
+    if (count == 0) return ASTRO_OK;  // an empty batch may pass null arrays
+    if (!cons || !x) return ASTRO_E_INVALID;
     k_c2p_features<<<grid_for(count, 256), 256, 0, (cudaStream_t)stream>>>(cons, x, count);
     mark(2, (cudaStream_t)stream);
     return cuda_status(cudaGetLastError());

@@ -258,8 +258,9 @@ int astro_mlp_trainable(void) { return kTrainable; }
 
 int astro_mlp_forward(const void* params, const float* x, float* y, int64_t n, int* status,
                       void* stream) {
-    if (!params || !x || !y || n < 0) return ASTRO_E_INVALID;
-    if (n == 0) return ASTRO_OK;
+    if (!params || n < 0) return ASTRO_E_INVALID;
+    if (n == 0) return ASTRO_OK;  // an empty batch may pass null arrays
+    if (!x || !y) return ASTRO_E_INVALID;
     const long ntiles = (n + TILE - 1) / TILE;
     const int grid = (int)(ntiles < 4L * sm_count() ? ntiles : 4L * sm_count());
     k_mlp_forward<<<grid, TILE, kInferSmem + 16, (cudaStream_t)stream>>>((const Params*)params, x, y,

@@ -230,7 +230,8 @@ int astro_outflow_yz(double* pr, const AstroGrid* g, int ng, void* stream);
 /* --- pointwise conversions ----------------------------------------------
  * Array forms of prim_to_cons / cons_to_prim (core/srhd_core.py:47,62) and
  * prim_to_cons_rmhd / cons_to_prim_rmhd (core/rmhd_core.py:138,249).
- * Arrays are (nm, count) float64. */
+ * Arrays are (nm, count) float64.  For these and the batch calls below a
+ * count of 0 does nothing and returns ASTRO_OK, with null arrays allowed. */
 int astro_p2c(const AstroParams* p, const double* prim, double* cons, int64_t count,
               void* stream);
 int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t count,

@@ -67,6 +67,25 @@ def test_error_strings_and_validation(lib):
     assert lib.astro_rhs_workspace_bytes(C.byref(p), C.byref(g)) == 0
 
 
+def test_empty_batches_are_no_ops(lib):
+    """A count of 0 returns ASTRO_OK before any device work, null arrays
+    allowed; a positive count with null arrays or a negative count is
+    rejected on the host."""
+    p = _lib.AstroParams()
+    p.physics, p.recon, p.riemann = 1, 2, 2
+    p.gamma = p.srhd_gamma = 4.0 / 3.0
+    assert lib.astro_p2c(C.byref(p), None, None, 0, None) == 0
+    assert lib.astro_c2p(C.byref(p), None, None, 0, None, None) == 0
+    assert lib.astro_c2p_learned(C.byref(p), None, None, 0, 2, None, 0, None, None, None) == 0
+    assert lib.astro_c2p_features(None, None, 0, None) == 0
+    assert lib.astro_mlp_forward(C.c_void_p(8), None, None, 0, None, None) == 0
+    assert lib.astro_p2c(C.byref(p), None, None, 4, None) == -1
+    assert lib.astro_c2p(C.byref(p), None, None, -1, None, None) == -1
+    assert lib.astro_c2p_learned(C.byref(p), None, None, 4, 2, None, 0, None, None, None) == -1
+    assert lib.astro_c2p_features(None, None, -2, None) == -1
+    assert lib.astro_mlp_forward(None, None, None, 0, None, None) == -1
+
+
 def test_product_raises_without_gpu_instead_of_falling_back():
     import torch
     if torch.cuda.is_available():
