@@ -84,15 +84,16 @@ CASES = [
 ]
 
 # Non-cubic blocks (the x-slabs of the reference's MPI driver have unequal
-# extents), with dx = 1/nx, dy = 1/ny, dz = 1/nz all different, and blocks one
-# interior cell thick in one direction.
+# extents), with dx = 1/nx, dy = 1/ny, dz = 1/nz all different, and blocks
+# with a single updated layer in one direction.
 CASES += [
     _c("s_muscl_mc_hllc_ragged", "srhd", "muscl", "mc", "hllc", 3, 2, seed=121, n=(5, 9, 7)),
     _c("s_weno_hlle_ragged", "srhd", "weno", "mc", "hlle", 2, 3, seed=122, n=(9, 4, 6)),
     _c("s_ppm_hlle_ragged_pass1", "srhd", "ppm", "mc", "hlle", 3, 3, n_extra=1, seed=123,
        n=(6, 7, 5)),
+    # SRHD MUSCL updates [2, n-3): of two interior x cells only the first
     _c("s_muscl_minmod_hlle_thin", "srhd", "muscl", "minmod", "hlle", 2, 2, seed=124,
-       n=(1, 6, 5)),
+       n=(2, 6, 5)),
     _c("r_weno_hlld_ragged", "rmhd", "weno", "mc", "hlld", 3, 3, seed=221, n=(6, 10, 5)),
     _c("r_muscl_mc_hlle_ragged_resist", "rmhd", "muscl", "mc", "hlle", 2, 2, seed=222,
        n=(11, 5, 8), RESISTIVE_ENABLED=True, RESISTIVITY=1e-3),
