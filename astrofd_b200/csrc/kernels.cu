@@ -165,7 +165,10 @@ int validate(const AstroParams* p, const AstroGrid* g) {
         return ASTRO_E_SHAPE;
     // the bulk pressure the SRHD MUSCL faces add sits in variable 5
     if (p->physics == ASTRO_SRHD && p->passive_offset > 5 && g->nv < 6) return ASTRO_E_SHAPE;
-    if (g->nx < 8 || g->ny < 8 || g->nz < 8) return ASTRO_E_SHAPE;
+    // any block size: where a small block leaves a scheme's cell range
+    // [lo, n - off) empty, nothing is updated there, as in the reference's
+    // loops; every stencil read of a cell in the range stays inside the block
+    if (g->nx < 1 || g->ny < 1 || g->nz < 1) return ASTRO_E_SHAPE;
     // cell indices are 32-bit in the kernels; 2^31 cells of even 5 float64
     // variables exceed the device memory
     if ((double)g->nx * g->ny * g->nz >= 2147483648.0) return ASTRO_E_SHAPE;
@@ -870,8 +873,9 @@ void launch_face_dir(const FaceArgs& a, bool given, dim3 grd, dim3 blk, cudaStre
 
 template <typename R>
 cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
-    const long total = (long)a.ext[0] * a.ext[1] * a.ext[2];
-    if (total <= 0) return cudaSuccess;
+    // an empty cell range in any direction: no faces (checked per extent,
+    // since two negative extents would give a positive product)
+    if (a.ext[0] <= 0 || a.ext[1] <= 0 || a.ext[2] <= 0) return cudaSuccess;
     const unsigned plane = (unsigned)a.ext[1] * (unsigned)a.ext[2];
     const dim3 blk(128), grd((plane + 127) / 128, (unsigned)(a.ext[0] < 65535 ? a.ext[0] : 65535));
     const AstroParams& p = a.p;
