@@ -1,0 +1,118 @@
+"""Properties checked at the measured configurations' full sizes, where the
+oracle is too slow to compare cell by cell: the C4 con2prim batch of 2^24
+states and the 256^3 magnetised jet of the benchmark (11 variables, NG 3,
+WENO5 + "hlld", mixed precision, learned con2prim, conservative fluxes)."""
+import numpy as np
+import pytest
+import torch
+
+from astrofd_b200 import learned_c2p as LC
+from astrofd_b200.core import rmhd_core
+from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
+
+pytestmark = pytest.mark.gpu
+
+N_C4 = 1 << 24
+N_JET, NG = 256, 3
+
+
+def _perpendicular(prim):
+    """B projected perpendicular to v: the reference's residual then has one
+    physical root, so any start that converges lands on its solution."""
+    v, b = prim[1:4], prim[5:8]
+    b -= v * (np.sum(v * b, axis=0) / np.maximum(np.sum(v * v, axis=0), 1e-300))
+    return prim
+
+
+def test_c4_full_batch_learned_equals_reference_con2prim():
+    """All 2^24 states of the C4 sampler (v.B = 0) through the learned path
+    with the shipped network agree with the reference's con2prim (the device
+    kernel the parity tests pin to the reference) to the solver's tolerance:
+    rho and |v| within 1e-5 relative, p within 1e-8 max(1, tau), on all but
+    1e-3 of the states, and the fields pass through unchanged."""
+    e = LC.c2p_engine()
+    prim = _perpendicular(LC.sample_primitives(N_C4, 2024))
+    U = e.p2c_array(torch.as_tensor(prim, device="cuda"))
+    del prim
+    ref = e.c2p_array(U)
+    params = torch.as_tensor(LC.load(), dtype=torch.float32).cuda()
+    q, st = LC.c2p_learned(e, U, params, max_polish=2)
+    assert st["status"] == 0 and st["cells"] == N_C4
+    assert st["learned_polish"] + st["learned_fallback"] == N_C4
+    assert torch.equal(q[5:], ref[5:])
+    ok = torch.isfinite(ref).all(0)
+    assert ok.double().mean().item() > 0.999
+    assert torch.isfinite(q[:, ok]).all()
+    d_rho = (q[0] - ref[0]).abs() / ref[0].abs()
+    d_v = (q[1:4] - ref[1:4]).norm(dim=0) / ref[1:4].norm(dim=0).clamp_min(1e-300)
+    d_p = (q[4] - ref[4]).abs() / U[4].clamp_min(1.0)
+    off = ((torch.maximum(d_rho, d_v) > 1e-5) | (d_p > 1e-8)) & ok
+    assert off.double().mean().item() < 1e-3
+
+
+def _jet_block():
+    """The benchmark's 256^3 ambient block with a jet cylinder of radius 0.1
+    along x (rho 0.1, v 0.99, toroidal field): strong shear layers, and the
+    con2prim fallback in use."""
+    pr = rmhd_jet(N_JET, NG)
+    N = N_JET + 2 * NG
+    y = (np.arange(N) - NG + 0.5) / N_JET - 0.5
+    yy, zz = np.meshgrid(y, y, indexing="ij")
+    r = np.sqrt(yy ** 2 + zz ** 2)
+    core = r < 0.1
+    pr[0][:, core] = 0.1
+    pr[1][:, core] = 0.99
+    pr[6][:, core] = (-0.5 * zz / 0.1)[core]
+    pr[7][:, core] = (0.5 * yy / 0.1)[core]
+    return torch.from_numpy(pr).cuda()
+
+
+def _configure():
+    core, _, _ = rmhd_jet_config(N_JET, NG, boundaries="baseline")
+    rmhd_core.configure(dict(core, PRECISION="mixed", C2P_GUESS="learned",
+                             FLUX_MODE="conservative"))
+    rmhd_core.set_c2p_network(LC.load())
+    return core
+
+
+def test_256_stagewise_equals_one_call_step():
+    """The three SSPRK3 stages called one at a time (astro_step_stage) give
+    the one-call step (astro_step) bit for bit on the benchmark block."""
+    core = _configure()
+    pr = _jet_block()
+    d = 1.0 / N_JET
+    dt = core["CFL"] * d
+    ref = rmhd_core.step_ssprk3(pr, d, d, d, dt)
+    bufs = [torch.empty_like(pr) for _ in range(3)]
+    cur = pr
+    for st in range(3):
+        rmhd_core.step_stage(pr, cur, bufs[st], d, d, d, dt, 3, st)
+        cur = bufs[st]
+    assert torch.isfinite(cur).all()
+    assert torch.equal(cur, ref)
+
+
+def test_256_conservative_step_conserves_mass():
+    """Conservative fluxes telescope: with the medium at rest and uniform in
+    the outer 16 cells of every face (one SSPRK3 step of WENO5 stages reaches
+    9 cells), no mass crosses the faces of the update region, and sum(rho W)
+    over the block changes only by the con2prim tolerance of the cells
+    (|f| < 1e-10 max(1, tau)) and float64 summation."""
+    core = _configure()
+    pr = _jet_block()
+    w = 16
+    amb = pr[:, 0, 0, 0].clone()
+    amb[1:4] = 0.0  # the ambient state (uniform Bx, passives) at rest
+    for sl in (np.s_[:, :w], np.s_[:, -w:], np.s_[:, :, :w], np.s_[:, :, -w:],
+               np.s_[:, :, :, :w], np.s_[:, :, :, -w:]):
+        pr[sl] = amb.view(-1, 1, 1, 1)
+
+    def mass(q):
+        v2 = q[1] ** 2 + q[2] ** 2 + q[3] ** 2
+        return (q[0] / torch.sqrt(1.0 - v2)).sum().item()
+
+    d = 1.0 / N_JET
+    m0 = mass(pr)
+    out = rmhd_core.step_ssprk3(pr, d, d, d, 0.2 * d)
+    assert torch.isfinite(out).all()
+    assert abs(mass(out) - m0) / m0 < 1e-10
