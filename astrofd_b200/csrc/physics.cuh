@@ -887,19 +887,31 @@ AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, do
     // 1/(Z+B^2)^2, 1/(1-v^2), Z/(rho W^2)) and one square root: the same
     // residual to rounding, far inside the Newton tolerance
     const double G = P.gamma, SM = 1e-12;
-    const double iZ = 1.0 / rmax(Z, SM);
-    const double vb = SB * iZ;
+    const double Zf = rmax(Z, SM);
     const double ZpB = Z + B2;
     const double Bq = ZpB * ZpB + SM;
-    const double iBq = 1.0 / Bq;
+    // 1/Z and 1/(Z+B^2)^2 from one division (of their product), unless the
+    // product leaves the float64 range
+    double iZ, iBq;
+    const double ZB = Zf * Bq;
+    if (ZB < 1e300) {
+        const double t = 1.0 / ZB;
+        iZ = t * Bq;
+        iBq = t * Zf;
+    } else {
+        iZ = 1.0 / Zf;
+        iBq = 1.0 / Bq;
+    }
+    const double vb = SB * iZ;
     double v2 = (S2 + (SB * SB) * (2.0 * Z + B2) * (iZ * iZ)) * iBq;
     const double vmax2 = P.v_max * P.v_max;
     const bool vcap = v2 >= vmax2;
     if (vcap) v2 = vmax2 - 1e-14;
-    const double om = 1.0 - v2;  // 1 / W^2
-    const double W2 = 1.0 / om;
-    const double rho = D * sqrt(om);  // D / W, W >= 1
-    const double h = Z / rmax(rho * W2, SM);
+    const double om = 1.0 - v2;  // 1 / W^2 >= 1 - v_max^2 > 0
+    const double W = rsqrt(om);
+    const double W2 = W * W;
+    const double rho = D * (om * W);  // D / W, W >= 1
+    const double h = Z / rmax(D * W, SM);  // rho W^2 = D W
     const double gm = (G - 1.0) / G;
     double p = (h - 1.0) * rho * gm;
     bool pcap = false;
@@ -962,10 +974,20 @@ AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U
     double Bx = U[5], By = U[6], Bz = U[7];
     double B2 = Bx * Bx + By * By + Bz * Bz;
     double SB = Sx * Bx + Sy * By + Sz * Bz;
-    // divisions regrouped as in r_f_df_of_Z (same values to rounding)
+    // divisions regrouped as in r_f_df_of_Z (same values to rounding): 1/Z
+    // and 1/(Z+B^2) from one division unless their product leaves the range
     double ZpB = Z + B2;
-    double vb = SB * (1.0 / rmax(Z, SM));
-    const double iZB = 1.0 / rmax(ZpB, SM);
+    const double Zf = rmax(Z, SM), ZBf = rmax(ZpB, SM);
+    double iZ, iZB;
+    if (Zf * ZBf < 1e300) {
+        const double t = 1.0 / (Zf * ZBf);
+        iZ = t * ZBf;
+        iZB = t * Zf;
+    } else {
+        iZ = 1.0 / Zf;
+        iZB = 1.0 / ZBf;
+    }
+    double vb = SB * iZ;
     double vx = (Sx + vb * Bx) * iZB;
     double vy = (Sy + vb * By) * iZB;
     double vz = (Sz + vb * Bz) * iZB;
@@ -976,8 +998,9 @@ AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U
         vx *= fac; vy *= fac; vz *= fac;
     }
     const double om = 1.0 - (vx * vx + vy * vy + vz * vz);  // 1 / W^2
-    double rho = D * sqrt(om);                               // D / W, W >= 1
-    double h = Z / rmax(rho / om, SM);
+    const double W = rsqrt(om);
+    double rho = D * (om * W);                               // D / W, W >= 1
+    double h = Z / rmax(D * W, SM);                          // rho / om = D W
     double p = (h - 1.0) * rho * ((G - 1.0) / G);
     if (!isfinite(rho) || !isfinite(p) || rho <= 0.0 || p <= 0.0) return false;
     q[0] = rho; q[1] = vx; q[2] = vy; q[3] = vz; q[4] = p;
