@@ -22,7 +22,8 @@ from states import make_state
 pytestmark = pytest.mark.gpu
 
 
-def _params(physics, recon, riemann, n_passive=0):
+def _params(physics, recon, riemann, n_passive=0, precision=_lib.PREC_FP64,
+            flux_mode=_lib.FLUX_REFERENCE):
     p = _lib.AstroParams()
     p.physics, p.recon, p.riemann, p.limiter = physics, recon, riemann, 0
     p.n_passive = n_passive
@@ -30,8 +31,8 @@ def _params(physics, recon, riemann, n_passive=0):
     p.gamma = 4.0 / 3.0 if physics == _lib.RMHD else 5.0 / 3.0
     p.srhd_gamma = 5.0 / 3.0
     p.p_max, p.v_max, p.glm_ch, p.glm_cp = 2.0, 0.9999, 1.0, 0.1
-    p.flux_mode = _lib.FLUX_REFERENCE
-    p.precision = _lib.PREC_FP64
+    p.flux_mode = flux_mode
+    p.precision = precision
     return p
 
 
@@ -44,14 +45,20 @@ def _with_workspace(L, p, g, pr, out, stream):
     assert rc == 0, L.astro_error_string(rc)
 
 
-@pytest.mark.parametrize("physics,recon,riemann,n_passive", [
-    (_lib.RMHD, 2, 1, 0),   # WENO5 + hlld, loop-carried x-face speeds
-    (_lib.SRHD, 0, 1, 2),   # MUSCL + HLLC with passive scalars
+@pytest.mark.parametrize("physics,recon,riemann,n_passive,precision,flux_mode", [
+    # WENO5 + hlld, loop-carried x-face speeds
+    (_lib.RMHD, 2, 1, 0, _lib.PREC_FP64, _lib.FLUX_REFERENCE),
+    # MUSCL + HLLC with passive scalars
+    (_lib.SRHD, 0, 1, 2, _lib.PREC_FP64, _lib.FLUX_REFERENCE),
+    # float32 faces: the float32 primitive copy and the counter of faces to
+    # redo in float64 also live in the shared scratch
+    (_lib.RMHD, 2, 1, 0, _lib.PREC_MIXED, _lib.FLUX_CONSERVATIVE),
 ])
-def test_static_scratch_rhs_matches_workspace_rhs(physics, recon, riemann, n_passive):
+def test_static_scratch_rhs_matches_workspace_rhs(physics, recon, riemann, n_passive,
+                                                  precision, flux_mode):
     L = _lib.load()
     stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    p = _params(physics, recon, riemann, n_passive)
+    p = _params(physics, recon, riemann, n_passive, precision, flux_mode)
     assert L.astro_rhs_static_max_bytes() == 32 << 20
     phys = "srhd" if physics == _lib.SRHD else "rmhd"
     nm = 5 if phys == "srhd" else 9
