@@ -86,6 +86,30 @@ def test_empty_batches_are_no_ops(lib):
     assert lib.astro_mlp_forward(None, None, None, 0, None, None) == -1
 
 
+def test_static_scratch_rhs_host_checks(lib):
+    """The allocation-free right-hand side checks its arguments on the host,
+    before it looks up its device scratch or launches anything: null arrays
+    are invalid, and a grid whose scratch would not fit the fixed 32 MiB
+    array is refused with ASTRO_E_WORKSPACE.  The non-null addresses below are
+    never dereferenced."""
+    cap = lib.astro_rhs_static_max_bytes()
+    assert cap == 32 << 20
+    p = _lib.AstroParams()
+    p.physics, p.recon, p.riemann = _lib.RMHD, 2, 1
+    p.passive_offset = 9
+    p.gamma = p.srhd_gamma = 4.0 / 3.0
+    g = _lib.AstroGrid(9, 22, 22, 22, 0.1, 0.1, 0.1)
+    assert 0 < lib.astro_rhs_workspace_bytes(C.byref(p), C.byref(g)) <= cap
+    assert lib.astro_rhs_static(C.byref(p), C.byref(g), None, None, None) == -1
+    g = _lib.AstroGrid(9, 134, 134, 134, 0.1, 0.1, 0.1)
+    assert lib.astro_rhs_workspace_bytes(C.byref(p), C.byref(g)) > cap
+    dummy = C.c_void_p(16)
+    assert lib.astro_rhs_static(C.byref(p), C.byref(g), dummy, dummy, None) == -3
+    # invalid parameters are reported before the size check
+    p.riemann = 7
+    assert lib.astro_rhs_static(C.byref(p), C.byref(g), dummy, dummy, None) == -1
+
+
 def test_product_raises_without_gpu_instead_of_falling_back():
     import torch
     if torch.cuda.is_available():
