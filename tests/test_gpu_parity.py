@@ -2,7 +2,7 @@
 against the reference's golden fixtures and the C oracle.
 
 Tolerances (normwise per variable, max|a-b| / max|ref|):
-  FP64 right-hand side         1e-10  (observed ~1e-12: FMA / fastmath rounding)
+  FP64 right-hand side         1e-11  (observed <= 2.7e-12 over the cases: FMA / fastmath rounding)
   FP64 step, hlle/hllc/hlld    1e-7   (con2prim stops at |f| < 1e-10 max(1,tau))
   FP64 step, hlld_full         1e-6 on cells the reference did not blow up
   mixed-precision rhs          5e-3   (float32 reconstruction + Riemann on the
@@ -51,7 +51,7 @@ def test_rhs_fp64_vs_reference(case):
     pr = torch.from_numpy(d["pr_in"]).to(DEV)
     r = _rhs_fn(m, case)(pr, *pr.shape[1:], *spacing(case)).cpu().numpy()
     assert r.shape == d["rhs"].shape
-    assert PT.normwise(r, d["rhs"]) < 1e-10
+    assert PT.normwise(r, d["rhs"]) < 1e-11
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
@@ -76,7 +76,7 @@ def test_numpy_inputs_round_trip_through_device(case):
     m = _mods(case)
     r = _rhs_fn(m, case)(d["pr_in"], *d["pr_in"].shape[1:], *spacing(case))
     assert isinstance(r, np.ndarray)
-    assert PT.normwise(r, d["rhs"]) < 1e-10
+    assert PT.normwise(r, d["rhs"]) < 1e-11
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
