@@ -53,7 +53,8 @@ class AstroNozzle(C.Structure):
                 ("ti", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
                 ("y0", C.c_double), ("z0", C.c_double),
                 ("tracer_nozzle", C.c_double * 8), ("tracer_amb", C.c_double * 8),
-                ("b_amb_x", C.c_double)]
+                ("b_amb_x", C.c_double), ("chemistry", C.c_int32),
+                ("chem_offset", C.c_int32), ("chem_x", C.c_double * 3)]
 
 
 class AstroChemistry(C.Structure):
@@ -80,7 +81,7 @@ GR_MINKOWSKI, GR_SCHWARZSCHILD, GR_KERR_SCHILD, GR_OTHER = 0, 1, 2, 3
 class AstroC2PStats(C.Structure):
     _fields_ = [(n, C.c_ulonglong) for n in
                 ("cells", "newton", "bisection", "hydro_fallback", "learned_polish",
-                 "learned_fallback", "polish_steps", "reserved")]
+                 "learned_fallback", "polish_steps", "tc_timeouts")]
 
 
 class AstroKernelTimes(C.Structure):
@@ -105,6 +106,7 @@ PROTOS = {
                                       C.c_double, C.c_int, _VP, C.c_size_t, _VP, _VP,
                                       C.POINTER(AstroKernelTimes)]),
     "astro_launch_count": (C.c_ulonglong, []),
+    "astro_debug_set_mma_poll_limit": (C.c_int, [C.c_longlong]),
     "astro_max_char_speed_workspace_bytes": (C.c_size_t, []),
     "astro_max_char_speed": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP,
                                        _DP, _VP, C.c_size_t, _VP]),

@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def build(verbose=False):
-    cmd = ["make", "-C", os.path.join(HERE, "csrc")]
+    cmd = ["make", "-j4", "-C", os.path.join(HERE, "csrc")]
     if not verbose:
         cmd.insert(1, "-s")
     subprocess.check_call(cmd)

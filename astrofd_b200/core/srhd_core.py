@@ -87,15 +87,31 @@ def step_stage(pr, pr_stage, out, dx, dy, dz, dt, rk_order, stage):
 
 
 def prim_to_cons(rho, vx, vy, vz, p, gamma=None):
-    """Scalars (as the reference) or equal-shaped arrays/tensors."""
-    return _pointwise(_E.p2c_array, (rho, vx, vy, vz, p))
+    """Scalars (as the reference) or equal-shaped arrays/tensors.  Without
+    ``gamma`` the reference's default applies: 5/3, bound when the module was
+    imported (core/srhd_core.py:47), whatever GAMMA is configured; an explicit
+    ``gamma`` is used for this call, as the reference honours it."""
+    return _pointwise(_E.p2c_array, (rho, vx, vy, vz, p), gamma)
 
 
 def cons_to_prim(D, Sx, Sy, Sz, tau, gamma=None):
-    return _pointwise(_E.c2p_array, (D, Sx, Sy, Sz, tau))
+    """Inverse of prim_to_cons, with the same ``gamma`` rule
+    (core/srhd_core.py:62)."""
+    return _pointwise(_E.c2p_array, (D, Sx, Sy, Sz, tau), gamma)
 
 
-def _pointwise(fn, comps):
+def _pointwise(fn, comps, gamma=None):
+    if gamma is None:
+        return _pointwise_call(fn, comps)
+    saved = _E.p.srhd_gamma
+    _E.p.srhd_gamma = float(gamma)
+    try:
+        return _pointwise_call(fn, comps)
+    finally:
+        _E.p.srhd_gamma = saved
+
+
+def _pointwise_call(fn, comps):
     import torch
     if isinstance(comps[0], torch.Tensor):
         shape = comps[0].shape

@@ -35,6 +35,12 @@ namespace {
 
 // process-wide count of kernels this library has launched (diagnostic only)
 std::atomic<unsigned long long> g_launches{0};
+// polls per MMA-completion wait of the learned con2prim (test hook)
+std::atomic<long long> g_mma_poll_limit{0};
+inline long mma_poll_limit() {
+    const long long v = g_mma_poll_limit.load(std::memory_order_relaxed);
+    return v > 0 ? (long)v : mlp::kPollLimit;
+}
 
 // Optional per-launch CUDA-event timing (astro_step_profiled, and the
 // astro_prof_start/stop sessions): an event is recorded after every launch;
@@ -308,20 +314,61 @@ __global__ void __launch_bounds__(128) k_face(FaceArgs a) {
     }
 }
 
+// whether everything face_at stored for this face (fluxes, and the speeds
+// and face velocities where the pass keeps them) is finite
+template <int NM>
+__device__ __forceinline__ bool face_stored_finite(const FaceArgs& a, size_t nc, size_t cell) {
+    bool ok = true;
+    const float* F = (const float*)a.F;
+#pragma unroll
+    for (int v = 0; v < NM; ++v) ok &= isfinite(F[(size_t)v * nc + cell]);
+    if (a.aux) {
+        const float* A = (const float*)a.aux;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) ok &= isfinite(A[(size_t)m * nc + cell]);
+    }
+    if (a.speeds_out) {
+        const float* S = (const float*)a.speeds_out;
+        ok &= isfinite(S[cell]) && isfinite(S[nc + cell]);
+    }
+    return ok;
+}
+
 // float64 recomputation of the faces a float32 pass listed as non-finite
 // (float32 overflows where float64 does not, e.g. squared WENO smoothness
-// indicators of a state whose fields have grown past ~1e9)
+// indicators of a state whose fields have grown past ~1e9).  If more faces
+// failed than the list holds (the counter keeps counting past its capacity),
+// the list is incomplete: every face of the pass is then checked and the
+// non-finite ones are recomputed, so no float32 failure is left in place.
 template <int PHYS, int RECON, int RIEMANN, bool GIVEN, int DIR>
 __global__ void __launch_bounds__(128) k_face_fix(FaceArgs a) {
-    const unsigned n = min(*a.fix_count, a.fix_cap);
-    for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
-        const long t = a.fix_list[q];
-        const int c = (int)(t % a.ext[2]);
-        const long r = t / a.ext[2];
-        const int bb = (int)(r % a.ext[1]);
-        const int aa = (int)(r / a.ext[1]);
-        face_at<PHYS, RECON, RIEMANN, double, float, GIVEN, DIR>(a, a.org[0] + aa, a.org[1] + bb,
-                                                                a.org[2] + c);
+    constexpr int NM = PHYS == ASTRO_SRHD ? 5 : 9;
+    const unsigned cnt = *a.fix_count;
+    if (cnt <= a.fix_cap) {
+        for (unsigned q = blockIdx.x * blockDim.x + threadIdx.x; q < cnt;
+             q += gridDim.x * blockDim.x) {
+            const long t = a.fix_list[q];
+            const int c = (int)(t % a.ext[2]);
+            const long r = t / a.ext[2];
+            const int bb = (int)(r % a.ext[1]);
+            const int aa = (int)(r / a.ext[1]);
+            face_at<PHYS, RECON, RIEMANN, double, float, GIVEN, DIR>(a, a.org[0] + aa,
+                                                                    a.org[1] + bb, a.org[2] + c);
+        }
+        return;
+    }
+    const size_t nc = (size_t)a.nx * a.ny * a.nz;
+    const size_t plane = (size_t)a.ext[1] * a.ext[2];
+    const size_t total = (size_t)a.ext[0] * plane;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const int aa = (int)(q / plane);
+        const size_t tp = q % plane;
+        const int bb = (int)(tp / a.ext[2]), c = (int)(tp % a.ext[2]);
+        const int i = a.org[0] + aa, j = a.org[1] + bb, k = a.org[2] + c;
+        const size_t cell = ((size_t)i * a.ny + j) * a.nz + k;
+        if (!face_stored_finite<NM>(a, nc, cell))
+            face_at<PHYS, RECON, RIEMANN, double, float, GIVEN, DIR>(a, i, j, k);
     }
 }
 
@@ -617,6 +664,7 @@ struct C2PArgs {
     unsigned* fb_count = nullptr;  // null: every cell is solved in k_c2p_learned
     unsigned* fb_list = nullptr;   // cell indices
     unsigned fb_cap = 0;
+    long poll_limit = mlp::kPollLimit;  // polls per MMA-completion wait
 };
 
 __device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell) {
@@ -640,7 +688,11 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + mlp::kInferSmem);
     uint32_t* taddr_s = reinterpret_cast<uint32_t*>(sm + mlp::kInferSmem + 8);
     const int t = threadIdx.x;
-    const bool net = a.net != nullptr;  // uniform; without a network: Z = D + tau + B^2
+    // uniform across the block; without a network: Z = D + tau + B^2.  If a
+    // tensor-core wait gives up, the block finishes its tiles without the
+    // network (same solver, analytic start), so no cell is left unsolved.
+    bool net = a.net != nullptr;
+    bool timed_out = false;
     if (net) {
         if (t < 32) mlp::tmem_alloc(mlp::smem_u32(taddr_s), 64);
         if (t == 0) mlp::mbar_init_fenced(mlp::smem_u32(bar), 1);
@@ -679,8 +731,10 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
             c2p_features(U, xr);
             mlp::features_norm(a.net, xr, h0);
             if (!mlp::forward_tile<false>(sm, tmem, mlp::smem_u32(bar), phase, a.net, h0, o,
-                                          a.status))
-                break;
+                                          a.status, a.poll_limit)) {
+                net = false;
+                timed_out = true;
+            }
         }
         if (!valid) continue;
         ++n_cells;
@@ -723,12 +777,14 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
 #pragma unroll
             for (int v = 0; v < 9; ++v) a.qf[(size_t)v * a.count + cell] = (float)q[v];
     }
-    if (net) {
+    if (a.net) {
+        if (timed_out) mlp::drain_after_timeout(mlp::smem_u32(bar), phase);
         mlp::tc_fence_before();
         __syncthreads();
         if (t < 32) mlp::tmem_free(tmem, 64);
     }
     if (a.stats) {
+        if (timed_out && t == 0) atomicAdd(&a.stats->tc_timeouts, 1ull);
         atomicAdd(&a.stats->cells, (unsigned long long)n_cells);
         if (n_polish) atomicAdd(&a.stats->learned_polish, (unsigned long long)n_polish);
         if (n_fallback) atomicAdd(&a.stats->learned_fallback, (unsigned long long)n_fallback);
@@ -848,15 +904,20 @@ __global__ void k_prim_f32(const double* __restrict__ pr, float* __restrict__ pr
 // direction is a template parameter so the per-direction component indices
 // fold to constants and the face state stays in registers
 template <int PH, int RE, int RI, typename R>
-void launch_face_dir(const FaceArgs& a, bool given, dim3 grd, dim3 blk, cudaStream_t s) {
+cudaError_t launch_face_dir(const FaceArgs& a, bool given, dim3 grd, dim3 blk, cudaStream_t s) {
     constexpr bool F32 = sizeof(R) == 4;
     const dim3 fgrd(148 * 4);
-    if (F32) cudaMemsetAsync(a.fix_count, 0, sizeof(unsigned), s);
+    // the fix-up counter starts every float32 pass at zero (the workspace, or
+    // the shared static scratch, holds the previous pass's count)
+    if (F32) {
+        const cudaError_t e = cudaMemsetAsync(a.fix_count, 0, sizeof(unsigned), s);
+        if (e != cudaSuccess) return e;
+    }
     if constexpr (PH == ASTRO_RMHD && RE != ASTRO_RECON_MUSCL) {
         if (given) {
             k_face<PH, RE, RI, R, true, 0><<<grd, blk, 0, s>>>(a);
             if (F32) k_face_fix<PH, RE, RI, true, 0><<<fgrd, blk, 0, s>>>(a);
-            return;
+            return cudaSuccess;
         }
     }
     if (a.dir == 0) {
@@ -869,6 +930,7 @@ void launch_face_dir(const FaceArgs& a, bool given, dim3 grd, dim3 blk, cudaStre
         k_face<PH, RE, RI, R, false, 2><<<grd, blk, 0, s>>>(a);
         if (F32) k_face_fix<PH, RE, RI, false, 2><<<fgrd, blk, 0, s>>>(a);
     }
+    return cudaSuccess;
 }
 
 template <typename R>
@@ -879,7 +941,8 @@ cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
     const unsigned plane = (unsigned)a.ext[1] * (unsigned)a.ext[2];
     const dim3 blk(128), grd((plane + 127) / 128, (unsigned)(a.ext[0] < 65535 ? a.ext[0] : 65535));
     const AstroParams& p = a.p;
-#define FACE(PH, RE, RI) launch_face_dir<PH, RE, RI, R>(a, given, grd, blk, s)
+    cudaError_t me = cudaSuccess;
+#define FACE(PH, RE, RI) me = launch_face_dir<PH, RE, RI, R>(a, given, grd, blk, s)
 #define RECONS(PH, RI)                                                          \
     do {                                                                        \
         if (p.recon == 0) FACE(PH, 0, RI);                                      \
@@ -896,6 +959,7 @@ cudaError_t launch_face_t(const FaceArgs& a, bool given, cudaStream_t s) {
     }
 #undef RECONS
 #undef FACE
+    if (me != cudaSuccess) return me;
     mark(0, s);
     return cudaGetLastError();
 }
@@ -1169,6 +1233,9 @@ __global__ void k_nozzle(double* pr, int nv, int nx, int ny, int nz, AstroNozzle
             pr[(size_t)c.thermo_offset * nc + cell] = c.te;
             pr[(size_t)(c.thermo_offset + 1) * nc + cell] = c.ti;
         }
+        // the inflow's ionisation fractions (core/nozzle.py:77-82)
+        if (c.chemistry && nv > c.chem_offset + 2)
+            for (int m = 0; m < 3; ++m) pr[(size_t)(c.chem_offset + m) * nc + cell] = c.chem_x[m];
         if (c.physics == 1) {
             double Bx = 0.0, By = 0.0, Bz = 0.0;
             if (c.b_init == 1) Bx = c.b0 * s;
@@ -1575,34 +1642,82 @@ int grid_for(size_t n, int block) {
 // Scratch for astro_rhs_static: a fixed-size array in the module's device
 // memory.  Every device that loads this library holds it (32 MiB) until the
 // process exits.  Host code must not use the symbol's name as a device
-// pointer: the device address is looked up once per device with
-// cudaGetSymbolAddress (with that device current) and cached here.
+// pointer: the device address is looked up with cudaGetSymbolAddress while
+// the caller's context is current, once per CUDA context, and cached under
+// that context's unique ID (cuCtxGetId, never reused within a process).  A
+// primary context re-created after cudaDeviceReset, or a driver-API context
+// the caller made current, is a new context with its own copy of the module,
+// so it gets its own lookup instead of a stale address.
 static constexpr size_t kStaticScratchBytes = size_t(32) << 20;
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 namespace {
-constexpr int kMaxDevices = 64;
-std::atomic<void*> g_static_scratch_addr[kMaxDevices];
+typedef int (*CtxGetCurrentFn)(void** ctx);
+typedef int (*CtxGetIdFn)(void* ctx, unsigned long long* id);
+
+struct ScratchEntry {
+    unsigned long long ctx_id;
+    void* ptr;
+};
+constexpr int kScratchEntries = 64;
+ScratchEntry g_scratch_cache[kScratchEntries];
+int g_scratch_used = 0, g_scratch_next = 0;
 std::mutex g_static_scratch_mu;
 
-// Device address of g_static_scratch on the current device (nullptr on error).
-void* static_scratch_address(int* err) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+// unique ID of the calling thread's current context, or 0 when the driver
+// entry points are unavailable (then every call looks the address up)
+unsigned long long current_context_id() {
+    static CtxGetCurrentFn get_cur = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_cur = (CtxGetCurrentFn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = (CtxGetIdFn)f;
+    });
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_cur || !get_id || get_cur(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
+
+// Device address of g_static_scratch in the current context (nullptr on
+// error).  The first call in a context may load the module; made while the
+// stream is being captured it is refused (ASTRO_E_INVALID), since a module
+// load inside a capture can invalidate it.
+void* static_scratch_address(cudaStream_t s, int* err) {
+    // a runtime call first, so that a thread with no current context gets the
+    // device's primary context before the driver is asked for it
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) {
         *err = ASTRO_E_CUDA;
         return nullptr;
     }
-    void* a = g_static_scratch_addr[dev].load(std::memory_order_acquire);
-    if (a) return a;
+    const unsigned long long id = current_context_id();
     std::lock_guard<std::mutex> lock(g_static_scratch_mu);
-    a = g_static_scratch_addr[dev].load(std::memory_order_acquire);
-    if (a) return a;
+    if (id != 0)
+        for (int e = 0; e < g_scratch_used; ++e)
+            if (g_scratch_cache[e].ctx_id == id) return g_scratch_cache[e].ptr;
+    if (cs != cudaStreamCaptureStatusNone) {
+        *err = ASTRO_E_INVALID;
+        return nullptr;
+    }
     void* ptr = nullptr;
     if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) {
         *err = ASTRO_E_CUDA;
         return nullptr;
     }
-    g_static_scratch_addr[dev].store(ptr, std::memory_order_release);
+    if (id != 0) {
+        int slot = g_scratch_used < kScratchEntries ? g_scratch_used++ : g_scratch_next;
+        if (slot == g_scratch_next) g_scratch_next = (g_scratch_next + 1) % kScratchEntries;
+        g_scratch_cache[slot] = ScratchEntry{id, ptr};
+    }
     return ptr;
 }
 }  // namespace
@@ -1686,6 +1801,7 @@ static int run_stage(const AstroParams* p, const AstroGrid* g, const Layout& L, 
         c.count = (long)g->nx * g->ny * g->nz;
         c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
         c.status = nullptr; c.max_polish = 2;
+        c.poll_limit = mma_poll_limit();
         c.fb_count = (unsigned*)(w + L.c2pfb);
         c.fb_list = (unsigned*)(w + L.c2pfb + 256);
         c.fb_cap = (unsigned)c2p_fb_capacity(*g);
@@ -1738,6 +1854,12 @@ int astro_step_stage(const AstroParams* p, const AstroGrid* g, const double* pr_
 }
 
 unsigned long long astro_launch_count(void) { return g_launches.load(); }
+
+int astro_debug_set_mma_poll_limit(long long polls) {
+    if (polls < 0) return ASTRO_E_INVALID;
+    g_mma_poll_limit.store(polls, std::memory_order_relaxed);
+    return ASTRO_OK;
+}
 
 int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* pr_in,
                         double* pr_out, double dt, int rk_order, void* work, size_t work_bytes,
@@ -1830,6 +1952,7 @@ int astro_nozzle_left_x(double* pr, const AstroGrid* g, const AstroNozzle* nz,
     if (nz->n_tracers > 0 && (nz->tracer_offset < 0 || nz->tracer_offset + nz->n_tracers > g->nv))
         return ASTRO_E_SHAPE;
     if (nz->two_temperature && nz->thermo_offset < 0) return ASTRO_E_SHAPE;
+    if (nz->chemistry && nz->chem_offset < 0) return ASTRO_E_SHAPE;
     if (nz->b_init < 0 || nz->b_init > 3 || nz->ambient_bc < 0 || nz->ambient_bc > 1)
         return ASTRO_E_INVALID;
     if (nz->ambient_bc == 1 && g->nx <= nz->ng) return ASTRO_E_SHAPE;
@@ -2044,6 +2167,7 @@ int astro_step_gr(const AstroParams* p, const AstroGrid* g, const AstroGR* gr,
             c.U = U; c.q = dst; c.count = (long)nc;
             c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
             c.status = nullptr; c.max_polish = 2;
+        c.poll_limit = mma_poll_limit();
             c.fb_count = (unsigned*)(w + L.c2pfb);
             c.fb_list = (unsigned*)(w + L.c2pfb + 256);
             c.fb_cap = (unsigned)c2p_fb_capacity(*g);
@@ -2091,6 +2215,7 @@ int astro_c2p_learned(const AstroParams* p, const double* cons, double* prim, in
     c.U = cons; c.q = prim; c.count = count; c.p = *p;
     c.net = (const mlp::Params*)p->mlp; c.stats = stats; c.status = status;
     c.max_polish = max_polish;
+    c.poll_limit = mma_poll_limit();
     if (work) {
         // fallback list: cell indices are 32-bit
         if (work_bytes < astro_c2p_learned_workspace_bytes(count)) return ASTRO_E_WORKSPACE;
@@ -2121,12 +2246,13 @@ int astro_rhs_static(const AstroParams* p, const AstroGrid* g, const double* pr,
     const Layout L = layout_of(*p, *g, false);
     if (L.total > kStaticScratchBytes) return ASTRO_E_WORKSPACE;  // grid too large
     int err = ASTRO_OK;
-    char* w = (char*)static_scratch_address(&err);
-    if (!w) return err;
     cudaStream_t s = (cudaStream_t)stream;
+    char* w = (char*)static_scratch_address(s, &err);
+    if (!w) return err;
     const Bounds b = bounds_of(*p, *g);
     // every scratch value the update reads is written by the face passes of
-    // this same call, so nothing has to be cleared first
+    // this same call; the one counter that must start at zero (the float32
+    // fix-up list's) is cleared by each face pass
     cudaError_t e = face_passes(*p, *g, b, pr, w, L, s);
     if (e != cudaSuccess) return ASTRO_E_CUDA;
     UpdArgs u = update_args(*p, *g, b, w, L);

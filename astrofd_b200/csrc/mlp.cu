@@ -38,7 +38,10 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const Params* P, const floa
         if (row < n)
             for (int i = 0; i < NIN; ++i) xr[i] = x[row * NIN + i];
         features_norm(P, xr, h0);
-        if (!forward_tile<false>(sm, tmem, smem_u32(bar), phase, P, h0, o, status)) break;
+        if (!forward_tile<false>(sm, tmem, smem_u32(bar), phase, P, h0, o, status)) {
+            drain_after_timeout(smem_u32(bar), phase);
+            break;
+        }
         if (row < n) {
             y[row * 2 + 0] = o[0] * P->ysd[0] + P->ymu[0];
             y[row * 2 + 1] = o[1] * P->ysd[1] + P->ymu[1];
@@ -113,7 +116,10 @@ __global__ void __launch_bounds__(128) k_mlp_train(const Params* P, const float*
         if (valid)
             for (int i = 0; i < NIN; ++i) xr[i] = x[row * NIN + i];
         features_norm(P, xr, h0);
-        if (!forward_tile<true>(sm, tmem, mbar, phase, P, h0, o, status)) break;
+        if (!forward_tile<true>(sm, tmem, mbar, phase, P, h0, o, status)) {
+            drain_after_timeout(mbar, phase);
+            break;
+        }
         // d(mean squared error)/d(output) in normalised target units
         float dy[16];
 #pragma unroll
@@ -171,7 +177,10 @@ __global__ void __launch_bounds__(128) k_mlp_train(const Params* P, const float*
             bool w = mbar_wait_bounded(mbar, phase, status);
             phase ^= 1u;
             ok = __syncthreads_and(w);
-            if (!ok) break;
+            if (!ok) {
+                drain_after_timeout(mbar, phase);
+                break;
+            }
             tc_fence_after();
             // weight gradient rows (out features) live in TMEM lanes 0..63
             if (warp < 2) {

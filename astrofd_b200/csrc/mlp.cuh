@@ -168,14 +168,44 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// polls of an MMA-completion wait before it gives up (~seconds)
+constexpr long kPollLimit = 1L << 26;
+
 // Bounded wait on the MMA-completion barrier.  Returns false (and records a
-// status) if the MMAs did not complete within the poll budget; the caller
-// then stops issuing work for this tile and exits cleanly.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, int* status) {
-    for (long it = 0; it < (1L << 26); ++it)
-        if (mbar_try_wait(mbar, parity)) return true;
+// status) if the MMAs did not complete within `limit` polls; the caller then
+// stops issuing work for this tile and exits cleanly.
+__device__ __forceinline__ bool mbar_test_wait(uint32_t mbar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t mbar, uint32_t parity, int* status,
+                                                  long limit = kPollLimit) {
+    if (limit < 1024) {
+        // a test limit of a few polls: non-blocking probes, since one
+        // try_wait may itself suspend the thread until the phase completes
+        for (long it = 0; it < limit; ++it)
+            if (mbar_test_wait(mbar, parity)) return true;
+    } else {
+        for (long it = 0; it < limit; ++it)
+            if (mbar_try_wait(mbar, parity)) return true;
+    }
     if (status) atomicExch(status, 1);
     return false;
+}
+
+// After a wait gave up at `phase` (already flipped by the caller), the MMAs
+// it waited for may still be running and writing TMEM: wait for them once
+// more, again bounded, before the block frees its TMEM and exits.
+__device__ __forceinline__ void drain_after_timeout(uint32_t mbar, uint32_t phase) {
+    mbar_wait_bounded(mbar, phase ^ 1u, nullptr);
 }
 
 // tanh.approx.f32: one MUFU operation; the PTX ISA bounds its relative error by
@@ -275,7 +305,8 @@ __device__ __forceinline__ void mma_kmajor(uint32_t tmem_d, uint32_t a_addr, int
 // Returns false if an MMA wait timed out (uniform across the block).
 template <bool TRAIN>
 __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, uint32_t mbar, uint32_t& phase,
-                             const Params* P, const float* h0, float* out, int* status) {
+                             const Params* P, const float* h0, float* out, int* status,
+                             long poll_limit = kPollLimit) {
     const int t = threadIdx.x;
     const int warp = t >> 5;
     const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
@@ -303,7 +334,7 @@ __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, u
                 mma_kmajor(tmem, a, 128, smem_u32(sm + OFF_W4), 16, NOUTP, 4);
             mma_commit(mbar);
         }
-        bool ok = mbar_wait_bounded(mbar, phase, status);
+        bool ok = mbar_wait_bounded(mbar, phase, status, poll_limit);
         phase ^= 1u;
         if (!__syncthreads_and(ok)) return false;
         tc_fence_after();

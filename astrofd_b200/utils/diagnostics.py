@@ -15,10 +15,12 @@ The reductions are one device kernel (astro_diagnostics) and one 48-byte
 copy back; the centreline is 5 x nx values copied back.  ``pr`` is a float64
 CUDA tensor (a numpy block is copied to the device first).
 
-``comm`` replaces the reference's mpi4py communicator: None for one
-process, or any object with ``allreduce(value, op)`` (op ``MAX`` or ``SUM``
-of this module) and ``gather(obj, root=0)``; ``TorchComm`` is that object
-over torch.distributed.  As in the reference, only rank 0 adds the inlet
+``comm`` is the reference's mpi4py communicator (the driver passes
+MPI.COMM_WORLD; reductions then use MPI.MAX / MPI.SUM, as
+utils/diagnostics.py:28,44 do), None for one process, or any other object
+with ``allreduce(value, op)`` (op ``MAX`` or ``SUM`` of this module) and
+``gather(obj, root=0)``; ``TorchComm`` is that object over
+torch.distributed.  As in the reference, only rank 0 adds the inlet
 plane (it holds the x = 0 slab) and writes the files.
 
 The reference calls prim_to_cons without an adiabatic index, so the module
@@ -67,8 +69,20 @@ class TorchComm:
         return out if self.rank == root else None
 
 
+def _comm_op(comm, op):
+    """``op`` in the communicator's own vocabulary: mpi4py's MPI.MAX /
+    MPI.SUM for an mpi4py communicator, this module's strings otherwise."""
+    if type(comm).__module__.split(".")[0] == "mpi4py":
+        import sys
+        mpi = sys.modules.get("mpi4py.MPI")
+        if mpi is None:
+            from mpi4py import MPI as mpi
+        return mpi.MAX if op == MAX else mpi.SUM
+    return op
+
+
 def _allreduce(comm, value, op):
-    return value if comm is None else comm.allreduce(value, op)
+    return value if comm is None else comm.allreduce(value, op=_comm_op(comm, op))
 
 
 def _gather(comm, obj):

@@ -84,8 +84,18 @@ def parse():
                     help="with --c2p-batch: states of a 128^3 jet run instead of the sampler")
     ap.add_argument("--validate-steps", type=int, default=0,
                     help="instead of timing: run this many steps of mixed+learned, plain "
-                         "float64 and float64 with a 1e-12 density perturbation and report "
-                         "density L1 errors and conservative-mode mass drift")
+                         "float64, float64 with a 1e-12 density perturbation and the two "
+                         "halves of the mixed+learned path (mixed faces with the "
+                         "reference's con2prim start, float64 faces with the learned "
+                         "start) in lockstep, and report density L1 errors against plain "
+                         "float64 and conservative-mode mass drift")
+    ap.add_argument("--validate-every", type=int, default=10,
+                    help="with --validate-steps: report the errors every this many steps")
+    ap.add_argument("--jet-v", type=float, default=0.995, help="jet three-velocity")
+    ap.add_argument("--sigma-jet", type=float, default=0.5,
+                    help="jet magnetisation (toroidal field); 0: unmagnetised jet")
+    ap.add_argument("--sigma-amb", type=float, default=0.01,
+                    help="ambient magnetisation (uniform Bx); 0: unmagnetised medium")
     return ap.parse_args()
 
 
@@ -617,44 +627,74 @@ def validate_srhd(args):
 
 
 def validate(args):
-    """Accuracy protocol of the mixed + learned path against plain float64."""
+    """Accuracy protocol of the mixed + learned path against plain float64.
+
+    Five runs of the same driver loop in lockstep: plain float64 (the
+    comparison), mixed + learned (the headline path), float64 with a 1e-12
+    relative density perturbation of the initial state (the floor: how far two
+    float64 runs drift apart on this flow), and the headline path's two halves
+    on their own: float32 faces with the reference's con2prim start, and
+    float64 faces with the learned start.  Relative L1 / Linf of rho, p and W
+    against plain float64 every --validate-every steps."""
     import torch
     from astrofd_b200 import learned_c2p
     from astrofd_b200.core import rmhd_core
     from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
     n, K = args.n, args.validate_steps
-    cfgs = rmhd_jet_config(n, 3, boundaries=args.boundaries)
+    cfgs = rmhd_jet_config(n, 3, vjet=args.jet_v, sigma_amb=args.sigma_amb,
+                           sigma_jet=args.sigma_jet, boundaries=args.boundaries)
     core, noz, src = cfgs
-
-    def run(prec, learned, perturb=0.0):
-        rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
-                                 C2P_GUESS="learned" if learned else "reference"))
-        if learned:
-            rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
-        pr = rmhd_jet(n, 3)
+    rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
+    arms = {"fp64": ("fp64", False, 0.0), "mixed_learned": ("mixed", True, 0.0),
+            "fp64_perturbed_1e-12": ("fp64", False, 1e-12),
+            "mixed_reference_guess": ("mixed", False, 0.0),
+            "fp64_learned_guess": ("fp64", True, 0.0)}
+    state = {}
+    for name, (prec, learned, perturb) in arms.items():
+        pr = rmhd_jet(n, 3, sigma_amb=args.sigma_amb)
         if perturb:
             pr[0] *= 1.0 + perturb * np.random.default_rng(5).standard_normal(pr[0].shape)
-        step = DriverStep(n, 3, core, noz, src)
         a = torch.from_numpy(pr).cuda()
-        b = torch.empty_like(a)
-        rmhd_core.c2p_stats(reset=True)
-        for _ in range(K):
-            a, b, _ = step(a, b)
-        return a, rmhd_core.c2p_stats(reset=True)
-
-    ref, st_ref = run("fp64", False)
-    mix, st_mix = run("mixed", True)
-    per, _ = run("fp64", False, perturb=1e-12)
-
-    nm, npr = _norms(mix, ref, 3), _norms(per, ref, 3)
+        state[name] = [a, torch.empty_like(a), DriverStep(n, 3, core, noz, src),
+                       {"cells": 0, "learned_fallback": 0, "hydro_fallback": 0,
+                        "tc_timeouts": 0}]
+    every = max(1, args.validate_every)
+    history = []
+    for k in range(1, K + 1):
+        for name, (prec, learned, _) in arms.items():
+            rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
+                                     C2P_GUESS="learned" if learned else "reference"))
+            st = state[name]
+            rmhd_core.c2p_stats(reset=True)
+            st[0], st[1], _ = st[2](st[0], st[1])
+            for key, v in rmhd_core.c2p_stats(reset=True).items():
+                if key in st[3]:
+                    st[3][key] += v
+        if k % every == 0 or k == K:
+            ref = state["fp64"][0]
+            rec = {"step": k}
+            for name in arms:
+                if name != "fp64":
+                    rec[name] = _norms(state[name][0], ref, 3)["rho"]["l1"]
+            history.append(rec)
+    ref = state["fp64"][0]
+    nm = _norms(state["mixed_learned"][0], ref, 3)
+    npr = _norms(state["fp64_perturbed_1e-12"][0], ref, 3)
     out = {"validate_steps": K, "grid": n, "flux_mode": args.flux_mode,
-           "boundaries": args.boundaries,
+           "boundaries": args.boundaries, "jet_v": args.jet_v, "sigma_jet": args.sigma_jet,
+           "sigma_amb": args.sigma_amb,
            "rho_l1_mixed_learned_vs_fp64": nm["rho"]["l1"],
            "rho_l1_fp64_perturbed_1e-12_vs_fp64": npr["rho"]["l1"],
+           "rho_l1_mixed_reference_guess_vs_fp64":
+               _norms(state["mixed_reference_guess"][0], ref, 3)["rho"]["l1"],
+           "rho_l1_fp64_learned_guess_vs_fp64":
+               _norms(state["fp64_learned_guess"][0], ref, 3)["rho"]["l1"],
            "mixed_learned_vs_fp64": nm, "fp64_perturbed_1e-12_vs_fp64": npr,
-           "c2p_fp64": st_ref, "c2p_mixed_learned": st_mix}
-    # mass: one conservative step of the same state with nothing crossing the
-    # faces of the update region (ambient at rest there) keeps sum(D) to round-off
+           "rho_l1_history": history,
+           "c2p_counts": {name: state[name][3] for name in arms}}
+    # mass: sum(D) of the conserved state, before and after one conservative
+    # float64 step of a state with nothing crossing the faces of the update
+    # region (ambient at rest there)
     rmhd_core.configure(dict(core, PRECISION="fp64", FLUX_MODE="conservative",
                              C2P_GUESS="reference"))
     a = torch.from_numpy(rmhd_jet(n, 3)).cuda()

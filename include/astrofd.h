@@ -17,8 +17,11 @@
  *     (astro_error_string() describes it).  Numerical failures inside kernels
  *     (con2prim falling back, iteration caps) never trap: they are counted in
  *     AstroC2PStats.
- *   - Thread safety: no mutable global state; calls on different streams are
- *     independent.
+ *   - Thread safety: calls on different streams are independent, with two
+ *     exceptions that share process-wide state: astro_rhs_static, whose
+ *     scratch is one array in the library's device memory shared by every
+ *     call on a device, and the astro_prof_start/stop and
+ *     astro_debug_set_mma_poll_limit settings.
  */
 #ifndef ASTROFD_B200_H
 #define ASTROFD_B200_H
@@ -101,6 +104,9 @@ typedef struct AstroNozzle {
     double dy, dz, y0, z0;
     double tracer_nozzle[8], tracer_amb[8];
     double b_amb_x;             /* axial ambient field carried through the inlet (b_init 3) */
+    int32_t chemistry;          /* CHEMISTRY_ENABLED: the inflow carries the       */
+    int32_t chem_offset;        /* ionisation fractions chem_x (xHII, xHeII,       */
+    double chem_x[3];           /* xHeIII) at variables chem_offset.. +2            */
 } AstroNozzle;
 
 /* con2prim outcome counters accumulated by astro_step/astro_c2p */
@@ -112,7 +118,10 @@ typedef struct AstroC2PStats {
     unsigned long long learned_polish; /* learned guess converged within <=2 steps  */
     unsigned long long learned_fallback; /* learned guess failed -> full solve      */
     unsigned long long polish_steps;   /* total polish steps taken                  */
-    unsigned long long reserved;
+    unsigned long long tc_timeouts;    /* learned guess: thread blocks whose tensor-
+                                          core wait gave up; they finished their
+                                          cells from Z = D + tau + B^2 instead, so
+                                          the result is still the full solve's      */
 } AstroC2PStats;
 
 /* --- build / diagnostics ------------------------------------------------ */
@@ -138,12 +147,16 @@ int astro_rhs(const AstroParams* p, const AstroGrid* g, const double* pr, double
  * (32 MiB) in the library's device memory, held by every GPU that loads the
  * library until the process exits.  Grids whose scratch would exceed it are
  * rejected with ASTRO_E_WORKSPACE (e.g. up to ~48^3 cells including ghosts
- * for RMHD WENO in float64 reference mode).  The first call on each device
- * looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make that first call before any stream capture.  All calls
- * share the one array: calls that overlap on the GPU (different streams or
- * host threads without ordering) race and must be serialised by the caller.
- * It calls no cudaMalloc/cudaFree. */
+ * for RMHD WENO in float64 reference mode).  The first call in each CUDA
+ * context (each device's primary context, one re-created after
+ * cudaDeviceReset, or a driver-API context the caller made current) looks up
+ * the array's device address there (cudaGetSymbolAddress, which may load the
+ * library's device code) and caches it under that context; make that first
+ * call before any stream capture: made on a capturing stream it returns
+ * ASTRO_E_INVALID.  All calls on a device share the one array, which keeps
+ * the last call's contents: calls that overlap on the GPU (different streams
+ * or host threads without ordering) race and must be serialised by the
+ * caller.  It calls no cudaMalloc/cudaFree. */
 size_t astro_rhs_static_max_bytes(void);
 int astro_rhs_static(const AstroParams* p, const AstroGrid* g, const double* pr, double* rhs,
                      void* stream);
@@ -191,6 +204,13 @@ int astro_step_profiled(const AstroParams* p, const AstroGrid* g, const double* 
 /* Number of kernels this library has launched in the process so far
  * (a diagnostic counter; no counterpart in the reference). */
 unsigned long long astro_launch_count(void);
+/* Test hook, no counterpart in the reference: polls each tensor-core
+ * completion wait of the learned con2prim makes before giving up, for the
+ * launches that follow (0 restores the default of 2^26, about a second).
+ * A small limit makes the waits give up while the MMAs are still running;
+ * the kernels then finish without the network and wait for those MMAs
+ * before freeing their tensor memory. */
+int astro_debug_set_mma_poll_limit(long long polls);
 /* No reference counterpart: kernel-class times over any sequence of this
  * library's calls, without host synchronisation in between.
  * astro_prof_start records an event on `stream`, then one after each of the

@@ -1315,6 +1315,8 @@ typedef struct {
     double vx_amb, vy_amb, vz_amb, turb_vamp, turb_pamp, b0, te, ti;
     double tracer_nozzle[8], tracer_amb[8];
     double b_amb_x;
+    int chemistry, chem_offset;  /* CHEMISTRY_ENABLED, CHEM_OFFSET         */
+    double chem_x[3];            /* CHEM_X_HII/HEII/HEIII_NOZZLE           */
 } ONozzle;
 
 static double nozzle_weight(double r, double radius, double shear, int profile) {
@@ -1375,6 +1377,9 @@ long oracle_nozzle_left_x(double* pr, int nv, int nx, int ny, int nz, double dy,
                     P(c->thermo_offset, gg, j, k) = c->te;
                     P(c->thermo_offset + 1, gg, j, k) = c->ti;
                 }
+                /* nozzle.py:77-82: the inflow's ionisation fractions */
+                if (c->chemistry && nv > c->chem_offset + 2)
+                    for (int m = 0; m < 3; ++m) P(c->chem_offset + m, gg, j, k) = c->chem_x[m];
                 if (c->physics == 1) {
                     double Bx = 0.0, By = 0.0, Bz = 0.0;
                     if (c->b_init == 1) Bx = c->b0 * s;

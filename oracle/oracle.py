@@ -60,7 +60,9 @@ class ONozzle(C.Structure):
                 ("vz_amb", C.c_double), ("turb_vamp", C.c_double),
                 ("turb_pamp", C.c_double), ("b0", C.c_double), ("te", C.c_double),
                 ("ti", C.c_double), ("tracer_nozzle", C.c_double * 8),
-                ("tracer_amb", C.c_double * 8), ("b_amb_x", C.c_double)]
+                ("tracer_amb", C.c_double * 8), ("b_amb_x", C.c_double),
+                ("chemistry", C.c_int), ("chem_offset", C.c_int),
+                ("chem_x", C.c_double * 3)]
 
 
 _lib = None
@@ -270,6 +272,10 @@ def nozzle_struct(cfg):
     c.b0 = cfg.get("B0", 0.0)
     c.te = float(cfg.get("TE_NOZZLE", cfg.get("TE_AMB", 0.0)) or 0.0)
     c.ti = float(cfg.get("TI_NOZZLE", cfg.get("TI_AMB", 0.0)) or 0.0)
+    c.chemistry = 1 if cfg.get("CHEMISTRY_ENABLED", False) else 0
+    c.chem_offset = int(cfg.get("CHEM_OFFSET", 0))
+    for m, key in enumerate(("CHEM_X_HII_NOZZLE", "CHEM_X_HEII_NOZZLE", "CHEM_X_HEIII_NOZZLE")):
+        c.chem_x[m] = float(cfg.get(key, 0.0))
     nv = cfg.get("TRACER_NOZZLE_VALUES", []) or []
     av = cfg.get("TRACER_AMB_VALUES", []) or []
     for t in range(min(c.n_tracers, 8)):

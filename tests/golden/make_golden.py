@@ -26,7 +26,7 @@ import numpy as np  # noqa: E402
 from cases import CASES, CASE_BY_NAME, DT_FRACTION, GR_CASES, GR_BY_NAME, spacing, step_dt  # noqa: E402
 import states  # noqa: E402
 
-SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
+SPECIAL = ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor", "bc_rmhd_chem",
            "c2p_rmhd", "c2p_srhd", "source_terms", "c1_run", "c5_run", "chemistry",
            "dissipation", "diagnostics", "gr_metric"]
 
@@ -114,6 +114,16 @@ def _bc_setup(name):
         cfg.update(NG=3, PHYSICS="rmhd", B_INIT="poloidal", B0=0.05,
                    NOZZLE_PROFILE="taper")
         seed = 5
+    elif name == "bc_rmhd_chem":
+        # ion chemistry on: the inflow carries the nozzle's ionisation
+        # fractions (nozzle.py:77-82) at CHEM_OFFSET, after Te/Ti
+        pr = states.make_state(305, 10, 3, "rmhd", n_extra=5)
+        cfg.update(NG=3, PHYSICS="rmhd", B_INIT="toroidal", B0=0.2, TWO_TEMPERATURE=True,
+                   THERMO_OFFSET=9, TE_NOZZLE=0.1, TI_NOZZLE=0.08, CHEMISTRY_ENABLED=True,
+                   CHEM_OFFSET=11, CHEM_X_HII_NOZZLE=0.9, CHEM_X_HEII_NOZZLE=0.05,
+                   CHEM_X_HEIII_NOZZLE=0.01, SHEAR_THICK=0.03, NOZZLE_PERTURB="random",
+                   TURB_VAMP=0.01, TURB_PAMP=0.01)
+        seed = 11
     else:  # bc_rmhd_tor
         pr = states.make_state(304, 10, 2, "rmhd", n_extra=2)
         cfg.update(NG=2, PHYSICS="rmhd", B_INIT="toroidal", B0=0.3,

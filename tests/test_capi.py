@@ -38,7 +38,7 @@ def test_struct_sizes_match_header_layout():
     assert C.sizeof(_lib.AstroParams) == 12 * 4 + 7 * 8
     assert C.sizeof(_lib.AstroGrid) == 4 * 4 + 3 * 8
     assert C.sizeof(_lib.AstroC2PStats) == 8 * 8
-    assert C.sizeof(_lib.AstroNozzle) == 10 * 4 + 18 * 8 + 16 * 8 + 8
+    assert C.sizeof(_lib.AstroNozzle) == 10 * 4 + 18 * 8 + 16 * 8 + 8 + 2 * 4 + 3 * 8
     assert C.sizeof(_lib.AstroChemistry) == 2 * 4 + 7 * 8
     assert C.sizeof(_lib.AstroDissipation) == 2 * 4 + 8 * 8
     assert C.sizeof(_lib.AstroGR) == 4 * 4 + 2 * 8

@@ -161,3 +161,35 @@ def test_two_x_slabs_over_gloo_equal_one_block(tmp_path):
     assert _read(run1, "centerline") == str(G["rmhd_centerline_csv"])
     assert len(_read(run1, "diagnostics").splitlines()) == 2
     assert [o["res"] for o in outs][0] == [o["res"] for o in outs][1]
+
+
+def test_mpi4py_communicator_gets_mpi_ops(monkeypatch):
+    """The reference's driver passes MPI.COMM_WORLD (utils/diagnostics.py:28,44
+    reduce with MPI.MAX / MPI.SUM): an mpi4py communicator receives mpi4py's
+    op objects, other communicators this module's MAX / SUM."""
+    import types
+    mpi = types.ModuleType("mpi4py.MPI")
+    mpi.MAX, mpi.SUM = object(), object()
+    seen = []
+
+    class Comm:
+        def allreduce(self, value, op=None):
+            seen.append(op)
+            return value
+
+    Comm.__module__ = "mpi4py.MPI"
+    pkg = types.ModuleType("mpi4py")
+    pkg.MPI = mpi
+    monkeypatch.setitem(sys.modules, "mpi4py", pkg)
+    monkeypatch.setitem(sys.modules, "mpi4py.MPI", mpi)
+    assert D._allreduce(Comm(), 2.0, D.MAX) == 2.0
+    assert D._allreduce(Comm(), 3.0, D.SUM) == 3.0
+    assert seen[0] is mpi.MAX and seen[1] is mpi.SUM
+
+    class Other:
+        def allreduce(self, value, op=None):
+            seen.append(op)
+            return value
+
+    D._allreduce(Other(), 1.0, D.MAX)
+    assert seen[-1] == D.MAX

@@ -123,6 +123,18 @@ def test_c2p_p2c_batches():
     assert rel.max() < 1e-2
 
 
+def test_srhd_conversions_honour_an_explicit_gamma():
+    """prim_to_cons / cons_to_prim (core/srhd_core.py:47,62) use an explicit
+    gamma; without one, the import-time default 5/3."""
+    from astrofd_b200.core import srhd_core
+    srhd_core.configure({})
+    U = srhd_core.prim_to_cons(1.0, 0.0, 0.0, 0.0, 1.0, gamma=4.0 / 3.0)
+    assert U[4] == pytest.approx(3.0, rel=1e-15)  # h = 1 + 4 p / rho
+    q = srhd_core.cons_to_prim(*U, gamma=4.0 / 3.0)
+    assert q[0] == pytest.approx(1.0, rel=1e-12) and q[4] == pytest.approx(1.0, rel=1e-9)
+    assert srhd_core.prim_to_cons(1.0, 0.0, 0.0, 0.0, 1.0)[4] == pytest.approx(1.5, rel=1e-15)
+
+
 def test_scalar_helpers_use_the_device():
     from astrofd_b200.core import srhd_core
     srhd_core.configure({})
@@ -132,7 +144,8 @@ def test_scalar_helpers_use_the_device():
     assert q[0] == pytest.approx(1.0, rel=1e-12) and q[4] == pytest.approx(1.0, rel=1e-9)
 
 
-@pytest.mark.parametrize("name", ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor"])
+@pytest.mark.parametrize("name", ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
+                                  "bc_rmhd_chem"])
 def test_ghost_fill(name):
     from astrofd_b200.core import boundary, nozzle
     d = PT.load(name)

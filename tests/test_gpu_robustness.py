@@ -1,0 +1,109 @@
+"""Recovery paths of the float32 faces and of the learned con2prim, through
+the C ABI on the device.
+
+* More non-finite float32 faces than the float64 fix-up list holds (its
+  capacity is nc/16 + 1024 faces per pass): every face of the pass is then
+  checked and the failed ones recomputed in float64, so the mixed right-hand
+  side still matches the float64 one instead of keeping NaN fluxes.
+* A tensor-core wait of the learned con2prim that gives up (made to give up
+  here by a poll limit of one poll, while the MMAs are still running): the
+  thread block finishes its cells from the analytic start, waits for the MMAs
+  still in flight before freeing its tensor memory, and the step counts the
+  event in AstroC2PStats.tc_timeouts; the primitives are the full solve's.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import parity as PT
+from astrofd_b200 import _lib, learned_c2p as LC
+from astrofd_b200.core import rmhd_core
+from astrofd_b200.workloads import rmhd_jet, rmhd_jet_config
+from states import make_state
+
+pytestmark = pytest.mark.gpu
+
+
+def _rmhd_params(precision):
+    p = _lib.AstroParams()
+    p.physics, p.recon, p.riemann, p.limiter = _lib.RMHD, 2, 1, 0
+    p.passive_offset = 9
+    p.gamma = p.srhd_gamma = 4.0 / 3.0
+    p.p_max, p.v_max, p.glm_ch, p.glm_cp = 1e60, 0.9999, 1.0, 0.1
+    p.flux_mode = _lib.FLUX_CONSERVATIVE
+    p.precision = precision
+    return p
+
+
+def _rhs(L, p, pr):
+    nv, nx, ny, nz = pr.shape
+    g = _lib.AstroGrid(nv, nx, ny, nz, 1 / 20, 1 / 20, 1 / 20)
+    nb = L.astro_rhs_workspace_bytes(C.byref(p), C.byref(g))
+    w = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    out = torch.full((9, nx, ny, nz), float("nan"), dtype=torch.float64, device="cuda")
+    rc = L.astro_rhs(C.byref(p), C.byref(g), C.c_void_p(pr.data_ptr()),
+                     C.c_void_p(out.data_ptr()), C.c_void_p(w.data_ptr()), nb, None)
+    assert rc == 0, L.astro_error_string(rc)
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def test_float32_fixup_list_overflow_recomputes_every_failed_face():
+    """Fields of ~1e12 with O(1) relative jumps: the squared WENO smoothness
+    indicators (~1e24, squared again in the weights) overflow float32 on every
+    face while the fluxes (~B^2) still fit, so all ~3 x 20^3 faces fail, far
+    more than the list's 1024 + 26^3/16 slots."""
+    L = _lib.load()
+    pr = make_state(41, 20, 3, "rmhd", noise=0.1, bamp=0.1, vjet=0.5, stripes=False)
+    rng = np.random.default_rng(3)
+    pr[5:8] = 1e12 * (1.0 + 0.5 * rng.random(pr[5:8].shape))
+    pr[4] = 1e20
+    t = torch.from_numpy(pr).cuda()
+    ref = _rhs(L, _rmhd_params(_lib.PREC_FP64), t)
+    got = _rhs(L, _rmhd_params(_lib.PREC_MIXED), t)
+    assert np.isfinite(ref).all()
+    assert np.isfinite(got).all()
+    # the recomputed fluxes are stored as float32: relative rounding ~1e-7
+    assert PT.normwise(got, ref) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_learned_con2prim_recovers_from_a_wait_that_gives_up(precision):
+    L = _lib.load()
+    N, NG = 24, 3
+    core, noz, _ = rmhd_jet_config(N, NG)
+    d = 1.0 / N
+    base = torch.from_numpy(rmhd_jet(N, NG)).cuda()
+    # a jet already inside the block
+    base[0, :NG + 4, N // 2 - 3:N // 2 + 3, N // 2 - 3:N // 2 + 3] = 0.1
+    base[1, :NG + 4, N // 2 - 3:N // 2 + 3, N // 2 - 3:N // 2 + 3] = 0.99
+
+    def step(guess):
+        rmhd_core.configure(dict(core, PRECISION=precision, FLUX_MODE="conservative",
+                                 C2P_GUESS=guess))
+        rmhd_core.set_c2p_network(LC.load())
+        rmhd_core.c2p_stats(reset=True)
+        out = rmhd_core.step_ssprk3(base.clone(), d, d, d, core["CFL"] * d)
+        torch.cuda.synchronize()
+        return out.cpu().numpy(), rmhd_core.c2p_stats(reset=True)
+
+    ref, st_ref = step("reference")
+    normal, st_normal = step("learned")
+    assert st_normal["tc_timeouts"] == 0
+    assert L.astro_debug_set_mma_poll_limit(1) == 0
+    try:
+        got, st = step("learned")
+    finally:
+        assert L.astro_debug_set_mma_poll_limit(0) == 0
+    assert st["tc_timeouts"] > 0, st
+    assert st["cells"] == st_normal["cells"]
+    assert np.isfinite(got).all()
+    tol = 1e-8 if precision == "fp64" else 1e-6
+    assert PT.normwise(got, ref) < tol
+    assert PT.normwise(got, normal) < tol
+    # the device still runs the network normally afterwards
+    again, st_again = step("learned")
+    assert st_again["tc_timeouts"] == 0
+    assert PT.normwise(again, normal) == 0.0

@@ -73,7 +73,8 @@ def test_c2p_rmhd():
     assert rel.max() < 1e-3
 
 
-@pytest.mark.parametrize("name", ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor"])
+@pytest.mark.parametrize("name", ["bc_srhd", "bc_srhd_tracers", "bc_rmhd_pol", "bc_rmhd_tor",
+                                  "bc_rmhd_chem"])
 def test_ghost_fill(name):
     d = PT.load(name)
     cfg = PT.params_of(d, "cfg")

@@ -90,3 +90,82 @@ def test_static_scratch_rejects_grids_beyond_its_size():
                             C.c_void_p(pr.data_ptr()), None)
     assert rc == -3
     assert L.astro_error_string(rc) == b"workspace missing or too small"
+
+
+def _static(L, p, g, pr, out, stream):
+    rc = L.astro_rhs_static(C.byref(p), C.byref(g), C.c_void_p(pr.data_ptr()),
+                            C.c_void_p(out.data_ptr()), stream)
+    assert rc == 0, L.astro_error_string(rc)
+
+
+@pytest.mark.parametrize("precision,flux_mode", [
+    (_lib.PREC_FP64, _lib.FLUX_REFERENCE), (_lib.PREC_MIXED, _lib.FLUX_CONSERVATIVE)])
+def test_static_scratch_large_grid_then_smaller_grids(precision, flux_mode):
+    """A grid whose scratch fills most of the array, then smaller ones: each
+    call's layout starts at the array's base, so the smaller calls read only
+    what they wrote, never the larger call's leftovers."""
+    L = _lib.load()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = _params(_lib.RMHD, 2, 1, 0, precision, flux_mode)
+    sizes = (40, 12, 25, 40)
+    first = None
+    for i, n in enumerate(sizes):
+        pr = torch.from_numpy(make_state(70 + i, n, 3, "rmhd", noise=0.1, bamp=0.1,
+                                         vjet=0.9, stripes=False)).cuda()
+        nv, nx, ny, nz = pr.shape
+        g = _lib.AstroGrid(nv, nx, ny, nz, 1 / n, 1 / n, 1 / n)
+        nb = L.astro_rhs_workspace_bytes(C.byref(p), C.byref(g))
+        if first is None:
+            first = nb
+            assert nb > (16 << 20)  # the large call uses over half of the array
+        ref = torch.zeros((9, nx, ny, nz), dtype=torch.float64, device="cuda")
+        got = torch.full_like(ref, float("nan"))
+        _with_workspace(L, p, g, pr, ref, stream)
+        _static(L, p, g, pr, got, stream)
+        torch.cuda.synchronize()
+        assert PT.normwise(got.cpu().numpy(), ref.cpu().numpy()) < 1e-10, n
+
+
+@pytest.mark.parametrize("name", ["r_weno_hlld_ragged", "s_muscl_mc_hllc_ragged"])
+def test_static_scratch_rhs_matches_reference_fixture(name):
+    """Against the right-hand side the reference itself computed (golden
+    fixture), at the float64 parity bar of the other right-hand-side tests."""
+    from astrofd_b200.core._engine import Engine
+    L = _lib.load()
+    d = PT.load(name)
+    params = PT.params_of(d)
+    phys = _lib.SRHD if name.startswith("s_") else _lib.RMHD
+    E = Engine(phys)
+    E.configure(dict(dict(RESISTIVE_ENABLED=False, RESISTIVITY=0.0, FLUX_MODE="reference",
+                          PRECISION="fp64"), **params))
+    pr = torch.from_numpy(d["pr_in"]).cuda()
+    nv, nx, ny, nz = pr.shape
+    ng = params["NG"]
+    g = _lib.AstroGrid(nv, nx, ny, nz, 1 / (nx - 2 * ng), 1 / (ny - 2 * ng), 1 / (nz - 2 * ng))
+    got = torch.full(d["rhs"].shape, float("nan"), dtype=torch.float64, device="cuda")
+    for _ in range(2):  # twice in a row on the shared scratch
+        _static(L, E.p, g, pr, got, None)
+        torch.cuda.synchronize()
+        assert PT.normwise(got.cpu().numpy(), d["rhs"]) < 1e-11
+
+
+@pytest.mark.skipif(not torch.cuda.is_available() or torch.cuda.device_count() < 2,
+                    reason="needs two GPUs")
+def test_static_scratch_on_a_second_device():
+    """Each device has its own copy of the array, looked up in its own
+    context: a call on device 1 after one on device 0 uses device 1's."""
+    L = _lib.load()
+    p = _params(_lib.RMHD, 2, 1)
+    for dev in (0, 1, 0):
+        with torch.cuda.device(dev):
+            pr = torch.from_numpy(make_state(80 + dev, 12, 3, "rmhd", noise=0.1, bamp=0.1,
+                                             vjet=0.9, stripes=False)).cuda()
+            nv, nx, ny, nz = pr.shape
+            g = _lib.AstroGrid(nv, nx, ny, nz, 1 / 12, 1 / 12, 1 / 12)
+            stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+            ref = torch.zeros((9, nx, ny, nz), dtype=torch.float64, device="cuda")
+            got = torch.full_like(ref, float("nan"))
+            _with_workspace(L, p, g, pr, ref, stream)
+            _static(L, p, g, pr, got, stream)
+            torch.cuda.synchronize()
+            assert PT.normwise(got.cpu().numpy(), ref.cpu().numpy()) < 1e-10
