@@ -28,7 +28,8 @@ class AstroParams(C.Structure):
                 ("riemann", C.c_int32), ("n_passive", C.c_int32),
                 ("passive_offset", C.c_int32), ("resistive", C.c_int32),
                 ("flux_mode", C.c_int32), ("precision", C.c_int32),
-                ("c2p_guess", C.c_int32), ("mlp", C.c_void_p), ("gamma", C.c_double),
+                ("c2p_guess", C.c_int32), ("split_stage", C.c_int32),
+                ("mlp", C.c_void_p), ("gamma", C.c_double),
                 ("srhd_gamma", C.c_double), ("p_max", C.c_double),
                 ("v_max", C.c_double), ("glm_ch", C.c_double), ("glm_cp", C.c_double),
                 ("resistivity", C.c_double)]
@@ -81,7 +82,7 @@ GR_MINKOWSKI, GR_SCHWARZSCHILD, GR_KERR_SCHILD, GR_OTHER = 0, 1, 2, 3
 class AstroC2PStats(C.Structure):
     _fields_ = [(n, C.c_ulonglong) for n in
                 ("cells", "newton", "bisection", "hydro_fallback", "learned_polish",
-                 "learned_fallback", "polish_steps", "tc_timeouts")]
+                 "learned_fallback", "polish_steps", "wait_timeouts")]
 
 
 class AstroKernelTimes(C.Structure):

@@ -89,6 +89,8 @@ class Engine:
         p.precision = _lib.PREC_MIXED if pm == "mixed" else _lib.PREC_FP64
         cg = str(g("C2P_GUESS", "reference")).lower()
         p.c2p_guess = _lib.GUESS_LEARNED if cg == "learned" else _lib.GUESS_REFERENCE
+        sk = str(g("STAGE_KERNEL", "split" if p.split_stage else "fused")).lower()
+        p.split_stage = 1 if sk == "split" else 0
 
     # -- right-hand side --------------------------------------------------
     def rhs(self, pr, nx, ny, nz, dx, dy, dz):

@@ -28,6 +28,7 @@
 
 #include "mlp.cuh"
 #include "physics.cuh"
+#include "stage.cuh"
 
 using namespace astro;
 
@@ -105,7 +106,10 @@ __host__ Bounds bounds_of(const AstroParams& p, const AstroGrid& g) {
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 struct Layout {
-    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, c2pfb, prf, total;
+    size_t prA, prB, U, F[3], FxC, aux[3], Sz, fix, c2pfb, prf, dfr, total;
+    bool fused;  // stages run as the fused kernel (stage.cu): no face buffers,
+                 // the float32 copy in padded rows of `pitch` floats
+    int pitch;
 };
 
 inline bool carried_mode(const AstroParams& p) {
@@ -131,16 +135,30 @@ inline size_t fix_capacity(const AstroGrid& g) {
 // warps; the listing kernel then carries no copy of the full solver
 inline size_t c2p_fb_capacity(const AstroGrid& g) { return (size_t)g.nx * g.ny * g.nz; }
 
-Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state) {
+// fused: the step's stages run as the fused kernel (astro_stage::supported;
+// steps only, not the GR wrappers)
+Layout layout_of(const AstroParams& p, const AstroGrid& g, bool with_state, bool fused = false) {
     Layout L;
+    memset(&L, 0, sizeof(L));
     const size_t nc = (size_t)g.nx * g.ny * g.nz;
     const int nm = p.physics == ASTRO_SRHD ? 5 : 9;
     const size_t rs = p.precision == ASTRO_PREC_MIXED ? 4 : 8;
     size_t o = 0;
     auto take = [&](size_t bytes) { size_t r = o; o += align256(bytes); return r; };
+    L.fused = fused && with_state;
+    L.pitch = g.nz;
     L.prA = with_state ? take((size_t)g.nv * nc * 8) : 0;
     L.prB = with_state ? take((size_t)g.nv * nc * 8) : 0;
     L.U = with_state ? take((size_t)nm * nc * 8) : 0;
+    if (L.fused) {
+        L.pitch = astro_stage::pitch_of(g.nz);
+        L.prf = take((size_t)nm * g.nx * g.ny * L.pitch * sizeof(float));
+        // cells whose float32 faces overflowed (a slot for every cell)
+        L.dfr = take(256 + nc * sizeof(unsigned));
+        L.c2pfb = p.c2p_guess == ASTRO_GUESS_LEARNED ? take(256 + c2p_fb_capacity(g) * sizeof(unsigned)) : 0;
+        L.total = o;
+        return L;
+    }
     for (int d = 0; d < 3; ++d) L.F[d] = take((size_t)nm * nc * rs);
     L.FxC = carried_mode(p) ? take((size_t)nm * nc * rs) : 0;
     for (int d = 0; d < 3; ++d) L.aux[d] = passive_fluxes(p) ? take(4 * nc * rs) : 0;
@@ -387,6 +405,8 @@ struct UpdArgs {
     double dd[3], dt;
     int stage, nstages, rhs_only;
     int defer_c2p;       // learned con2prim: write U every stage, primitives later
+    int frame_only;      // only the cells outside the updated range (the fused
+                         // stage kernel updates the others)
     AstroParams p;
     AstroC2PStats* stats;
 };
@@ -452,6 +472,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 8) k_update(UpdArg
         const unsigned i = r32 / (unsigned)a.ny;
         const bool in = (int)i >= a.b.lo && (int)i < a.b.hi[0] && (int)j >= a.b.lo &&
                         (int)j < a.b.hi[1] && (int)k >= a.b.lo && (int)k < a.b.hi[2];
+        if (DEFER && a.frame_only && in) return;
         const long st[3] = {(long)a.ny * a.nz, (long)a.nz, 1L};
         int nres = 0;
         if (PHYS == ASTRO_RMHD && a.p.resistive && a.p.resistivity > 0.0) {
@@ -655,6 +676,8 @@ struct C2PArgs {
     const double* U;   // [9][count]
     double* q;         // [>=9][count]: rows 0..8 written
     float* qf = nullptr;  // optional float32 copy of rows 0..8 (next stage's faces)
+    int qf_nz = 0, qf_pitch = 0;  // qf rows of qf_pitch floats per qf_nz cells
+                                  // (padded copy of the fused stages), else flat
     long count;
     AstroParams p;
     const mlp::Params* net;
@@ -666,6 +689,15 @@ struct C2PArgs {
     unsigned fb_cap = 0;
     long poll_limit = mlp::kPollLimit;  // polls per MMA-completion wait
 };
+
+// the float32 copy's index of (variable v, cell): flat, or rows padded to
+// qf_pitch floats
+__device__ __forceinline__ size_t qf_index(const C2PArgs& a, int v, long cell) {
+    if (a.qf_pitch == a.qf_nz) return (size_t)v * a.count + cell;
+    const unsigned c = (unsigned)cell, nz = (unsigned)a.qf_nz;
+    const size_t rows = (size_t)(a.count / a.qf_nz);
+    return ((size_t)v * rows + c / nz) * a.qf_pitch + c % nz;
+}
 
 __device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell) {
     if (!a.fb_list) return false;
@@ -775,7 +807,7 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
         if (a.qf)
 #pragma unroll
-            for (int v = 0; v < 9; ++v) a.qf[(size_t)v * a.count + cell] = (float)q[v];
+            for (int v = 0; v < 9; ++v) a.qf[qf_index(a, v, cell)] = (float)q[v];
     }
     if (a.net) {
         if (timed_out) mlp::drain_after_timeout(mlp::smem_u32(bar), phase);
@@ -784,7 +816,7 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
         if (t < 32) mlp::tmem_free(tmem, 64);
     }
     if (a.stats) {
-        if (timed_out && t == 0) atomicAdd(&a.stats->tc_timeouts, 1ull);
+        if (timed_out && t == 0) atomicAdd(&a.stats->wait_timeouts, 1ull);
         atomicAdd(&a.stats->cells, (unsigned long long)n_cells);
         if (n_polish) atomicAdd(&a.stats->learned_polish, (unsigned long long)n_polish);
         if (n_fallback) atomicAdd(&a.stats->learned_fallback, (unsigned long long)n_fallback);
@@ -811,7 +843,7 @@ __global__ void __launch_bounds__(128) k_c2p_fallback(C2PArgs a) {
         for (int v = 0; v < 9; ++v) a.q[(size_t)v * a.count + cell] = q[v];
         if (a.qf)
 #pragma unroll
-            for (int v = 0; v < 9; ++v) a.qf[(size_t)v * a.count + cell] = (float)q[v];
+            for (int v = 0; v < 9; ++v) a.qf[qf_index(a, (int)v, (long)cell)] = (float)q[v];
     }
     if (a.stats) {
         if (cnt.newton) atomicAdd(&a.stats->newton, (unsigned long long)cnt.newton);
@@ -898,6 +930,17 @@ __global__ void k_prim_f32(const double* __restrict__ pr, float* __restrict__ pr
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x)
         prf[i] = (float)pr[i];
+}
+
+// the same into rows padded to `pitch` floats (n = variables x nx x ny rows)
+__global__ void k_prim_f32_rows(const double* __restrict__ pr, float* __restrict__ prf, size_t rows,
+                                int nz, int pitch) {
+    const size_t n = rows * (size_t)nz;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i / (unsigned)nz, k = i % (unsigned)nz;
+        prf[r * pitch + k] = (float)pr[i];
+    }
 }
 
 // ------------------------------------------------------------- dispatch ---
@@ -1270,7 +1313,10 @@ __global__ void k_p2c(AstroParams p, const double* q, double* U, long count) {
     }
 }
 
-__global__ void k_c2p(AstroParams p, const double* U, double* q, long count, AstroC2PStats* stats) {
+// qf: optional float32 copy of the result in rows of `pitch` floats per nz
+// cells (the fused stages' input)
+__global__ void k_c2p(AstroParams p, const double* U, double* q, long count, AstroC2PStats* stats,
+                      float* qf = nullptr, int nz = 1, int pitch = 1) {
     const Phys<double> P = Phys<double>::from(p);
     C2PCount cnt;
     unsigned mine = 0;
@@ -1282,6 +1328,11 @@ __global__ void k_c2p(AstroParams p, const double* U, double* q, long count, Ast
         if (p.physics == ASTRO_SRHD) s_c2p(P, a, b);
         else r_c2p(P, a, b, cnt);
         for (int v = 0; v < nm; ++v) q[(size_t)v * count + t] = b[v];
+        if (qf) {
+            const size_t rows = (size_t)(count / nz);
+            const size_t r = (size_t)t / (unsigned)nz, k = (size_t)t % (unsigned)nz;
+            for (int v = 0; v < nm; ++v) qf[((size_t)v * rows + r) * pitch + k] = (float)b[v];
+        }
         ++mine;
     }
     if (stats) {
@@ -1760,9 +1811,14 @@ int astro_rhs(const AstroParams* p, const AstroGrid* g, const double* pr, double
     return cuda_status(launch_update(u, s));
 }
 
+// the layout of astro_step / astro_step_stage (fused stages where supported)
+static Layout step_layout(const AstroParams& p, const AstroGrid& g) {
+    return layout_of(p, g, true, astro_stage::supported(p, g));
+}
+
 size_t astro_step_workspace_bytes(const AstroParams* p, const AstroGrid* g) {
     if (validate(p, g) != ASTRO_OK) return 0;
-    return layout_of(*p, *g, true).total;
+    return step_layout(*p, *g).total;
 }
 
 // argument checks shared by astro_step and astro_step_stage
@@ -1774,16 +1830,78 @@ static int step_check(const AstroParams* p, const AstroGrid* g, int rk_order, vo
     const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
     if (p->c2p_guess != ASTRO_GUESS_REFERENCE && !learned) return ASTRO_E_INVALID;
     if (learned && (p->physics != ASTRO_RMHD || !p->mlp)) return ASTRO_E_UNSUPPORTED;
-    if (!work || work_bytes < layout_of(*p, *g, true).total) return ASTRO_E_WORKSPACE;
+    if (!work || work_bytes < step_layout(*p, *g).total) return ASTRO_E_WORKSPACE;
     return ASTRO_OK;
 }
 
 // One SSPRK stage: faces of cur, update (U_{st-1} -> U_st in the workspace),
 // con2prim into dst.  prf_ready: the float32 copy of cur is already in the
 // workspace; dstf: where the con2prim also writes dst's float32 copy.
+// The fused version: the float32 copy of cur (padded rows) if it is not in
+// the workspace yet, the fused kernel over the updated cells, the update of
+// the frame outside them, then con2prim of every cell (writing the next
+// stage's float32 copy).
+static int run_stage_fused(const AstroParams* p, const AstroGrid* g, const Layout& L, char* w,
+                           const double* pr_in, const double* cur, double* dst, double dt,
+                           int nst, int st, bool prf_ready, bool want_dstf,
+                           AstroC2PStats* stats, cudaStream_t s) {
+    const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
+    const Bounds b = bounds_of(*p, *g);
+    const size_t nc = (size_t)g->nx * g->ny * g->nz;
+    float* prf = (float*)(w + L.prf);
+    double* U = (double*)(w + L.U);
+    if (!prf_ready) {
+        k_prim_f32_rows<<<sm_count_cached() * 8, 256, 0, s>>>(cur, prf, (size_t)9 * g->nx * g->ny,
+                                                               g->nz, L.pitch);
+        mark(2, s);
+    }
+    astro_stage::StageArgs a;
+    memset(&a, 0, sizeof(a));
+    a.prf = prf; a.pr = cur; a.pr0 = pr_in; a.U = U; a.dst = dst;
+    a.timeouts = stats ? &stats->wait_timeouts : nullptr;
+    a.defer_count = (unsigned*)(w + L.dfr);
+    a.defer_list = (unsigned*)(w + L.dfr + 256);
+    a.nv = g->nv; a.nx = g->nx; a.ny = g->ny; a.nz = g->nz; a.pitch = L.pitch;
+    a.lo = b.lo; a.hi[0] = b.hi[0]; a.hi[1] = b.hi[1]; a.hi[2] = b.hi[2];
+    a.dd[0] = g->dx; a.dd[1] = g->dy; a.dd[2] = g->dz; a.dt = dt;
+    a.stage = st; a.nstages = nst; a.p = *p;
+    cudaError_t e = astro_stage::launch(a, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    mark(0, s);
+    UpdArgs u = update_args(*p, *g, b, w, L);
+    u.pr0 = pr_in; u.prk = cur; u.U = U; u.dst = dst; u.dstf = nullptr;
+    u.dt = dt; u.stage = st; u.nstages = nst; u.rhs_only = 0; u.stats = stats;
+    u.defer_c2p = 1; u.frame_only = 1;
+    e = launch_update(u, s);
+    if (e != cudaSuccess) return ASTRO_E_CUDA;
+    float* dstf = want_dstf ? prf : nullptr;
+    if (learned) {
+        C2PArgs c;
+        c.U = U; c.q = dst;
+        c.count = (long)nc;
+        c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
+        c.status = nullptr; c.max_polish = 2;
+        c.poll_limit = mma_poll_limit();
+        c.fb_count = (unsigned*)(w + L.c2pfb);
+        c.fb_list = (unsigned*)(w + L.c2pfb + 256);
+        c.fb_cap = (unsigned)c2p_fb_capacity(*g);
+        c.qf = dstf; c.qf_nz = g->nz; c.qf_pitch = L.pitch;
+        e = launch_c2p_learned(c, s);
+    } else {
+        k_c2p<<<sm_count_cached() * 8, 128, 0, s>>>(*p, U, dst, (long)nc, stats, dstf, g->nz,
+                                                    L.pitch);
+        mark(1, s);
+        e = cudaGetLastError();
+    }
+    return e == cudaSuccess ? ASTRO_OK : ASTRO_E_CUDA;
+}
+
 static int run_stage(const AstroParams* p, const AstroGrid* g, const Layout& L, char* w,
                      const double* pr_in, const double* cur, double* dst, double dt, int nst,
                      int st, bool prf_ready, float* dstf, AstroC2PStats* stats, cudaStream_t s) {
+    if (L.fused)
+        return run_stage_fused(p, g, L, w, pr_in, cur, dst, dt, nst, st, prf_ready,
+                               dstf != nullptr, stats, s);
     const bool learned = p->c2p_guess == ASTRO_GUESS_LEARNED;
     const Bounds b = bounds_of(*p, *g);
     cudaError_t e = face_passes(*p, *g, b, cur, w, L, s, prf_ready);
@@ -1818,7 +1936,7 @@ int astro_step(const AstroParams* p, const AstroGrid* g, const double* pr_in, do
     int v = step_check(p, g, rk_order, work, work_bytes);
     if (v != ASTRO_OK) return v;
     if (!pr_in || !pr_out || pr_in == pr_out) return ASTRO_E_INVALID;
-    const Layout L = layout_of(*p, *g, true);
+    const Layout L = step_layout(*p, *g);
     cudaStream_t s = (cudaStream_t)stream;
     char* w = (char*)work;
     const int nst = rk_order;
@@ -1846,7 +1964,7 @@ int astro_step_stage(const AstroParams* p, const AstroGrid* g, const double* pr_
     if (!pr_in || !pr_stage || !pr_out || pr_out == pr_in || pr_out == pr_stage)
         return ASTRO_E_INVALID;
     if (stage == 0 && pr_stage != pr_in) return ASTRO_E_INVALID;
-    const Layout L = layout_of(*p, *g, true);
+    const Layout L = step_layout(*p, *g);
     // the caller may have changed pr_stage's ghosts since it was written: the
     // float32 copy is made from it here
     return run_stage(p, g, L, (char*)work, pr_in, pr_stage, pr_out, dt, rk_order, stage, false,

@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--graph", action="store_true",
                     help="replay CUDA graphs of one driver iteration in the timed steps "
                          "(kernel-class times then come from profiled steps after them)")
+    ap.add_argument("--stage-kernel", default="fused", choices=["fused", "split"],
+                    help="fused: one kernel per SSPRK stage (TMA tiles, faces and update "
+                         "together); split: per-direction face passes, then the update")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -304,7 +307,7 @@ def time_arm(args, world, prec, pr_host, cfgs, profile, learned=False):
     from astrofd_b200.core import rmhd_core
     core, noz, src = cfgs
     cfg = dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
-               C2P_GUESS="learned" if learned else "reference")
+               C2P_GUESS="learned" if learned else "reference", STAGE_KERNEL=args.stage_kernel)
     rmhd_core.configure(cfg)
     if learned:
         from astrofd_b200 import learned_c2p
@@ -401,7 +404,8 @@ def time_e2e(args, world, prec, pr_host, cfgs, learned=False):
     from astrofd_b200.core import rmhd_core
     core, noz, src = cfgs
     rmhd_core.configure(dict(core, PRECISION=prec, FLUX_MODE=args.flux_mode,
-                             C2P_GUESS="learned" if learned else "reference"))
+                             C2P_GUESS="learned" if learned else "reference",
+                             STAGE_KERNEL=args.stage_kernel))
     if learned:
         from astrofd_b200 import learned_c2p
         rmhd_core.set_c2p_network(learned_c2p.load(args.c2p_net or learned_c2p.DATA))
@@ -657,7 +661,7 @@ def validate(args):
         a = torch.from_numpy(pr).cuda()
         state[name] = [a, torch.empty_like(a), DriverStep(n, 3, core, noz, src),
                        {"cells": 0, "learned_fallback": 0, "hydro_fallback": 0,
-                        "tc_timeouts": 0}]
+                        "wait_timeouts": 0}]
     every = max(1, args.validate_every)
     history = []
     for k in range(1, K + 1):

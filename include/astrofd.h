@@ -74,6 +74,11 @@ typedef struct AstroParams {
     int32_t physics, recon, limiter, riemann;
     int32_t n_passive, passive_offset, resistive, flux_mode;
     int32_t precision, c2p_guess;
+    int32_t split_stage; /* 0: SSPRK stages of RMHD WENO5/PPM with HLLE or
+                            "hlld", float32 faces and conservative fluxes run
+                            as one fused kernel per stage; 1: always the
+                            per-direction face passes + update (same result
+                            to float32 rounding)                           */
     const void* mlp;     /* device pointer to the learned-guess network's
                             parameter block (astro_mlp_param_bytes() bytes),
                             used when c2p_guess == ASTRO_GUESS_LEARNED        */
@@ -118,10 +123,13 @@ typedef struct AstroC2PStats {
     unsigned long long learned_polish; /* learned guess converged within <=2 steps  */
     unsigned long long learned_fallback; /* learned guess failed -> full solve      */
     unsigned long long polish_steps;   /* total polish steps taken                  */
-    unsigned long long tc_timeouts;    /* learned guess: thread blocks whose tensor-
-                                          core wait gave up; they finished their
-                                          cells from Z = D + tau + B^2 instead, so
-                                          the result is still the full solve's      */
+    unsigned long long wait_timeouts;  /* thread blocks whose bounded wait gave up:
+                                          a learned-guess block whose tensor-core
+                                          wait ran out finishes its cells from
+                                          Z = D + tau + B^2 (the result is still the
+                                          full solve's); a fused stage block whose
+                                          tile load never landed leaves its cells
+                                          unupdated (the step's result is invalid) */
 } AstroC2PStats;
 
 /* --- build / diagnostics ------------------------------------------------ */

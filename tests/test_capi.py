@@ -35,7 +35,8 @@ def test_every_declared_symbol_is_exported(lib):
 
 
 def test_struct_sizes_match_header_layout():
-    assert C.sizeof(_lib.AstroParams) == 12 * 4 + 7 * 8
+    # 11 int32 fields (padded to 12 before the pointer), the pointer, 7 doubles
+    assert C.sizeof(_lib.AstroParams) == 12 * 4 + 8 + 7 * 8
     assert C.sizeof(_lib.AstroGrid) == 4 * 4 + 3 * 8
     assert C.sizeof(_lib.AstroC2PStats) == 8 * 8
     assert C.sizeof(_lib.AstroNozzle) == 10 * 4 + 18 * 8 + 16 * 8 + 8 + 2 * 4 + 3 * 8
