@@ -52,9 +52,9 @@ constexpr int OFF_CNT = OFF_BAR + 8 * (NRING + 1);
 // one more mark word for the x faces
 constexpr int kYJobs = TY + 1;
 constexpr int kZJobs = (TY * (TZ + 1) + 31) / 32;
-constexpr int kJobs = kYJobs + kZJobs;
+constexpr int kJobs = kYJobs + kZJobs;  // y/z jobs; index kJobs is a warp's x row
 constexpr int OFF_FAIL = OFF_CNT + 4 * (NRING + 1);
-constexpr int kSmem = OFF_FAIL + 4 * 2 * kJobs;
+constexpr int kSmem = OFF_FAIL + 4 * 3 * kJobs;
 static_assert(OFF_RING % 128 == 0 && CORE_STRIDE * 4 % 128 == 0, "TMA alignment");
 static_assert(kSmem <= 56 * 1024, "four blocks per SM");
 constexpr long kPollLimit = 1L << 24;  // polls of a tile-load wait before it gives up
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (t < 2 * kJobs) failed[t] = 0;
+    if (t < 3 * kJobs) failed[t] = 0;
     __syncthreads();
     auto load_ring = [&](int pl) {
         const int s = slot_of(pl);
@@ -301,30 +301,33 @@ __global__ void __launch_bounds__(kThreads, 4)
         tma_load(smem_u32(halo), &tm_halo, k0 - 3, j0 - 3, pl, hbar);
         ++issued[NRING];
     };
-    if (t == 0) {
-        // the x faces' stencil of the first plane (planes i0-3 .. i0+2) and the
-        // first halo box
+    // the x faces' stencil of the first plane (planes i0-3 .. i0+2); the first
+    // halo box goes out after the pass for plane i0 - 1, like every later one
+    if (t == 0)
         for (int pl = i0 - 3; pl <= i0 + 2; ++pl) load_ring(pl);
-        load_halo(i0);
-    }
-    // planes i0-3 .. i0+1 here; the loop's first phase waits for i0+2
-    bool w = true;
-    for (int pl = i0 - 3; pl <= i0 + 1; ++pl) w &= bar_wait(bar0 + 8 * slot_of(pl), parity_of(pl));
-    bool ok = __syncthreads_and(w);
+    // planes i0-3 .. i0+1 here; the loop's first pass waits for i0+2
+    bool w0 = true;
+    for (int pl = i0 - 3; pl <= i0 + 1; ++pl) w0 &= bar_wait(bar0 + 8 * slot_of(pl), parity_of(pl));
+    bool ok = __syncthreads_and(w0);
 
     float Flo[NM], Fhi[NM];
-    // One loop over phases ph = 2 i + pass, so that the face code exists once:
-    // pass 0, the y and z faces of plane i (jobs from the halo box, fluxes to
-    // shared memory); pass 1, this thread's x face i + 1/2 (from the ring, to
-    // Fhi), then the update of the cells of plane i.  The first phase is pass
-    // 1 of plane i0 - 1: the x face i0 - 1/2.  A face whose float32 result is
-    // not finite is marked; the cells next to it are not updated here but
-    // listed for k_stage_fix, which redoes them with that face in float64.
+    // Per plane i, two barriers: (1) the waits for the halo box of plane i and
+    // ring plane i+3, which also separate the previous plane's update (reads
+    // of Fy / Fz) from this plane's face writes; (2) after the face jobs: the
+    // y and z faces of plane i from the halo box (fluxes to shared memory)
+    // and this thread's x face i + 1/2 from the ring (to Fhi), one loop so the
+    // face code exists once.  Then the next loads go out and the cells of
+    // plane i are updated.  The pass for "plane i0 - 1" computes only the x
+    // face i0 - 1/2.  A face whose float32 result is not finite is marked; the
+    // cells next to it are not updated here but listed for k_stage_fix, which
+    // redoes them with that face in float64.  Marks rotate over three buffers
+    // (written by plane i's jobs, read by its update, cleared during the next
+    // plane's update).
 #pragma unroll 1
-    for (int ph = 2 * i0 - 1; ph < 2 * i1 && ok; ++ph) {
-        const int i = ph >> 1, pass = ph & 1;
-        unsigned* fail = failed + (i & 1) * kJobs;  // this plane's marks
-        if (pass == 0 && mine) {
+    for (int i = i0 - 1; i < i1 && ok; ++i) {
+        unsigned* fail = failed + (i % 3) * kJobs;  // i >= 2: no negative modulo
+        const bool cells = i >= i0;
+        if (cells && mine) {
             // L2 prefetch of this cell's float64 update operands
             const size_t nc = (size_t)a.nx * a.ny * a.nz;
             const size_t cell = ((size_t)i * a.ny + j) * a.nz + k;
@@ -335,18 +338,19 @@ __global__ void __launch_bounds__(kThreads, 4)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + (size_t)v * nc + cell));
             }
         }
-        // also the barrier between the previous phase's reads of Fy / Fz / the
-        // ring and this phase's writes
-        ok = __syncthreads_and(pass == 0 ? bar_wait(hbar, (uint32_t)((i - i0) & 1))
-                                         : bar_wait(bar0 + 8 * slot_of(i + 3), parity_of(i + 3)));
+        bool w = bar_wait(bar0 + 8 * slot_of(i + 3), parity_of(i + 3));
+        if (cells) w &= bar_wait(hbar, (uint32_t)((i - i0) & 1));
+        ok = __syncthreads_and(w);
         if (!ok) break;
+        // jobs: y and z faces warp-strided (none for plane i0 - 1), then the
+        // warp's own x row
+        int job = cells ? warp : kJobs;
 #pragma unroll 1
-        for (int job = pass == 0 ? warp : kYJobs + kZJobs; job < kYJobs + kZJobs + pass;
-             job += TY) {
+        while (job <= kJobs) {
             const float* rows[6];
             int sv, dir, r, c;
             bool need;
-            if (job == kYJobs + kZJobs) {
+            if (job == kJobs) {
                 // x face of this thread's column, planes i-2 .. i+3 (every lane
                 // computes it; only the lanes that own a cell use it)
 #pragma unroll
@@ -378,56 +382,55 @@ __global__ void __launch_bounds__(kThreads, 4)
                 dir = 2;
                 need = f < TY * (TZ + 1) && j0 + r < a.hi[1] && k0 + c <= a.hi[2];
             }
-            if (!need) continue;
-            float F[NM];
-            const bool fin = face_any<RECON, RIEMANN>(P, lim, rows, sv, dir, F);
-            if (dir == 0) {
+            if (need) {
+                float F[NM];
+                const bool fin = face_any<RECON, RIEMANN>(P, lim, rows, sv, dir, F);
+                if (dir == 0) {
 #pragma unroll
-                for (int v = 0; v < NM; ++v) Fhi[v] = fin ? F[v] : __int_as_float(0x7fc00000);
-            } else if (dir == 1) {
+                    for (int v = 0; v < NM; ++v) Fhi[v] = fin ? F[v] : __int_as_float(0x7fc00000);
+                } else if (dir == 1) {
 #pragma unroll
-                for (int v = 0; v < NM; ++v) Fy[(v * (TY + 1) + r) * TZ + c] = F[v];
-                if (!fin) atomicOr(&fail[job], 1u << lane);
-            } else {
-#pragma unroll
-                for (int v = 0; v < NM; ++v) Fz[(v * TY + r) * (TZ + 1) + c] = F[v];
-                if (!fin) atomicOr(&fail[job], 1u << lane);
-            }
-        }
-        __syncthreads();  // this pass's inputs are consumed, its fluxes and marks complete
-        if (t == 0 && i + 1 < i1) {
-            if (pass == 0) load_halo(i + 1);
-            else load_ring(i + 4);
-        }
-        if (pass == 1) {
-            if (i >= i0 && mine) {
-                // the cell's y and z faces: marks, then fluxes
-                const int fz = warp * (TZ + 1) + lane;
-                const bool bad =
-                    !finite9(Flo) || !finite9(Fhi) || ((fail[warp] >> lane) & 1u) ||
-                    ((fail[warp + 1] >> lane) & 1u) ||
-                    ((fail[kYJobs + (fz >> 5)] >> (fz & 31)) & 1u) ||
-                    ((fail[kYJobs + ((fz + 1) >> 5)] >> ((fz + 1) & 31)) & 1u);
-                if (bad) {
-                    const unsigned slot = atomicAdd(a.defer_count, 1u);
-                    a.defer_list[slot] = (unsigned)(((size_t)i * a.ny + j) * a.nz + k);
+                    for (int v = 0; v < NM; ++v) Fy[(v * (TY + 1) + r) * TZ + c] = F[v];
+                    if (!fin) atomicOr(&fail[job], 1u << lane);
                 } else {
-                    float fyl[NM], fyh[NM], fzl[NM], fzh[NM];
 #pragma unroll
-                    for (int v = 0; v < NM; ++v) {
-                        fyl[v] = Fy[(v * (TY + 1) + warp) * TZ + lane];
-                        fyh[v] = Fy[(v * (TY + 1) + warp + 1) * TZ + lane];
-                        fzl[v] = Fz[v * TY * (TZ + 1) + fz];
-                        fzh[v] = Fz[v * TY * (TZ + 1) + fz + 1];
-                    }
-                    update_cell(a, i, j, k, Flo, Fhi, fyl, fyh, fzl, fzh);
+                    for (int v = 0; v < NM; ++v) Fz[(v * TY + r) * (TZ + 1) + c] = F[v];
+                    if (!fin) atomicOr(&fail[job], 1u << lane);
                 }
             }
-            // the next plane's marks (the other half), before its first pass
-            if (t < kJobs) failed[((i + 1) & 1) * kJobs + t] = 0;
-#pragma unroll
-            for (int v = 0; v < NM; ++v) Flo[v] = Fhi[v];
+            job = job == kJobs ? kJobs + 1 : (job + TY < kJobs ? job + TY : kJobs);
         }
+        __syncthreads();  // halo box and ring plane i-2 consumed; fluxes and marks complete
+        if (t == 0 && i + 1 < i1) {
+            load_halo(i + 1);
+            load_ring(i + 4);
+        }
+        if (cells && mine) {
+            // the cell's y and z faces: marks, then fluxes
+            const int fz = warp * (TZ + 1) + lane;
+            const bool bad = !finite9(Flo) || !finite9(Fhi) || ((fail[warp] >> lane) & 1u) ||
+                             ((fail[warp + 1] >> lane) & 1u) ||
+                             ((fail[kYJobs + (fz >> 5)] >> (fz & 31)) & 1u) ||
+                             ((fail[kYJobs + ((fz + 1) >> 5)] >> ((fz + 1) & 31)) & 1u);
+            if (bad) {
+                const unsigned slot = atomicAdd(a.defer_count, 1u);
+                a.defer_list[slot] = (unsigned)(((size_t)i * a.ny + j) * a.nz + k);
+            } else {
+                float fyl[NM], fyh[NM], fzl[NM], fzh[NM];
+#pragma unroll
+                for (int v = 0; v < NM; ++v) {
+                    fyl[v] = Fy[(v * (TY + 1) + warp) * TZ + lane];
+                    fyh[v] = Fy[(v * (TY + 1) + warp + 1) * TZ + lane];
+                    fzl[v] = Fz[v * TY * (TZ + 1) + fz];
+                    fzh[v] = Fz[v * TY * (TZ + 1) + fz + 1];
+                }
+                update_cell(a, i, j, k, Flo, Fhi, fyl, fyh, fzl, fzh);
+            }
+        }
+        // the marks of plane i + 2 (last read by the update of plane i - 1)
+        if (t < kJobs) failed[((i + 2) % 3) * kJobs + t] = 0;
+#pragma unroll
+        for (int v = 0; v < NM; ++v) Flo[v] = Fhi[v];
     }
     if (!ok) {
         // a tile load did not land in time: before the block's shared memory
