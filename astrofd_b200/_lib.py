@@ -28,7 +28,7 @@ class AstroParams(C.Structure):
                 ("riemann", C.c_int32), ("n_passive", C.c_int32),
                 ("passive_offset", C.c_int32), ("resistive", C.c_int32),
                 ("flux_mode", C.c_int32), ("precision", C.c_int32),
-                ("c2p_guess", C.c_int32), ("split_stage", C.c_int32),
+                ("c2p_guess", C.c_int32), ("fused_stage", C.c_int32),
                 ("mlp", C.c_void_p), ("gamma", C.c_double),
                 ("srhd_gamma", C.c_double), ("p_max", C.c_double),
                 ("v_max", C.c_double), ("glm_ch", C.c_double), ("glm_cp", C.c_double),

@@ -89,8 +89,10 @@ class Engine:
         p.precision = _lib.PREC_MIXED if pm == "mixed" else _lib.PREC_FP64
         cg = str(g("C2P_GUESS", "reference")).lower()
         p.c2p_guess = _lib.GUESS_LEARNED if cg == "learned" else _lib.GUESS_REFERENCE
-        sk = str(g("STAGE_KERNEL", "split" if p.split_stage else "fused")).lower()
-        p.split_stage = 1 if sk == "split" else 0
+        # STAGE_KERNEL (no reference counterpart): "split" (per-direction face
+        # passes + update, the default) or "fused" (one kernel per stage)
+        sk = str(g("STAGE_KERNEL", "fused" if p.fused_stage else "split")).lower()
+        p.fused_stage = 1 if sk == "fused" else 0
 
     # -- right-hand side --------------------------------------------------
     def rhs(self, pr, nx, ny, nz, dx, dy, dz):

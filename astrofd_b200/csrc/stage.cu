@@ -2,19 +2,24 @@
 //
 // Thread block: TY x TZ = 4 x 32 cells of a (y, z) column, 4 warps, warp w
 // owning row w.  The block marches along x over TX planes.  Per plane i:
-//   1. y and z faces of plane i from the halo box (TMA, 9 x 10 x 40 floats):
-//      (TY+1) rows of TZ y faces and TY rows of TZ+1 z faces, as jobs of 32
-//      faces with one direction each, spread over the warps; fluxes to shared
-//      memory.
-//   2. the x face i+1/2 of every cell of the column from the ring of the
-//      column's own cells (TMA, six planes i-2 .. i+3); flux in registers.
-//   3. per cell: divergence (x fluxes of i-1/2 and i+1/2 in registers, y and z
-//      fluxes from shared memory), GLM damping, resistive Laplacian, the
-//      float64 SSPRK combination; U_k to global memory.
-// While plane i's faces are computed, the halo box of plane i+1 and the ring
-// plane i+4 are in flight.  A float32 face whose result is not finite (float32
-// overflow) is recomputed in float64 from the float64 stage input, in place.
-// Cells outside [lo, hi)^3 (ghosts and the loop-bound frame) are not touched.
+//   1. wait for the halo box of plane i (TMA, 9 x 10 x 40 floats: the cells
+//      and their 3-cell y/z halo) and for ring plane i+3 (TMA, the column's
+//      own 4 x 36 cells of each of the six planes i-2 .. i+3);
+//   2. one loop of face jobs, 32 faces each: the (TY+1) rows of TZ y faces
+//      and the TY x (TZ+1) z faces from the halo box (fluxes to shared
+//      memory), spread over the warps, then each warp's own row of x faces
+//      i+1/2 from the ring (flux in registers).  The face code exists once:
+//      the vector components are rotated so every face is evaluated as an x
+//      face;
+//   3. barrier; the halo box of plane i+1 and ring plane i+4 go out;
+//   4. per cell: divergence (x fluxes of i-1/2 and i+1/2 in registers, y and z
+//      fluxes from shared memory), GLM damping, the resistive Laplacian (from
+//      the float32 tiles, differences in float64), the float64 SSPRK
+//      combination; U_k to global memory.
+// A float32 face whose result is not finite (float32 overflow) marks its two
+// cells: they are not updated here but listed, and k_stage_fix redoes them
+// with that face in float64 from the float64 stage input.  Cells outside
+// [lo, hi)^3 (ghosts and the loop-bound frame) are updated by the caller.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -164,9 +169,13 @@ __device__ __forceinline__ void face_f64(const StageArgs& a, int i, int j, int k
 // z): divergence, GLM damping, resistive Laplacian, the float64 SSPRK
 // combination (the split path's k_update, operation for operation), U_k and
 // the passive rows of dst.
+// lap: the cell's resistive Laplacian of B (3 values) when the caller has it
+// (the fused kernel, from its float32 tiles), else null: from the float64
+// stage input.
 __device__ __forceinline__ void update_cell(const StageArgs& a, int i, int j, int k,
                                             const float* fxl, const float* fxh, const float* fyl,
-                                            const float* fyh, const float* fzl, const float* fzh) {
+                                            const float* fyh, const float* fzl, const float* fzh,
+                                            const double* lap = nullptr) {
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
     const size_t cell = ((size_t)i * a.ny + j) * a.nz + k;
     const double i0d = 1.0 / a.dd[0], i1d = 1.0 / a.dd[1], i2d = 1.0 / a.dd[2];
@@ -181,7 +190,10 @@ __device__ __forceinline__ void update_cell(const StageArgs& a, int i, int j, in
     }
     const double* q = a.pr;
     rhs[8] -= a.p.glm_cp * a.p.glm_cp * q[8 * nc + cell];
-    if (a.p.resistive && a.p.resistivity > 0.0) {
+    if (a.p.resistive && a.p.resistivity > 0.0 && lap) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) rhs[5 + c] += a.p.resistivity * lap[c];
+    } else if (a.p.resistive && a.p.resistivity > 0.0) {
         const long sty = a.nz, stx = (long)a.ny * a.nz;
         const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
         const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
@@ -400,6 +412,27 @@ __global__ void __launch_bounds__(kThreads, 4)
             }
             job = job == kJobs ? kJobs + 1 : (job + TY < kJobs ? job + TY : kJobs);
         }
+        // the resistive Laplacian of B of this thread's cell from the tiles (the
+        // float32 copy; plane i in the halo box, planes i +- 1 in the ring),
+        // differences in float64 -- before the tiles are refilled
+        double lap[3];
+        const bool resist = a.p.resistive && a.p.resistivity > 0.0;
+        if (cells && mine && resist) {
+            const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
+            const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
+            const double iz2 = 1.0 / (a.dd[2] * a.dd[2] + 1e-12);
+            const float* hc = halo + (warp + 3) * HZ + lane + 3;
+            const float* rm = ring_at(i - 1) + warp * CZ + lane + 3;
+            const float* rp = ring_at(i + 1) + warp * CZ + lane + 3;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int v = 5 + c;
+                const double b0 = (double)hc[v * HY * HZ];
+                lap[c] = ((double)rp[v * TY * CZ] - 2.0 * b0 + (double)rm[v * TY * CZ]) * ix2 +
+                         ((double)hc[v * HY * HZ + HZ] - 2.0 * b0 + (double)hc[v * HY * HZ - HZ]) * iy2 +
+                         ((double)hc[v * HY * HZ + 1] - 2.0 * b0 + (double)hc[v * HY * HZ - 1]) * iz2;
+            }
+        }
         __syncthreads();  // halo box and ring plane i-2 consumed; fluxes and marks complete
         if (t == 0 && i + 1 < i1) {
             load_halo(i + 1);
@@ -424,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 4)
                     fzl[v] = Fz[v * TY * (TZ + 1) + fz];
                     fzh[v] = Fz[v * TY * (TZ + 1) + fz + 1];
                 }
-                update_cell(a, i, j, k, Flo, Fhi, fyl, fyh, fzl, fzh);
+                update_cell(a, i, j, k, Flo, Fhi, fyl, fyh, fzl, fzh, resist ? lap : nullptr);
             }
         }
         // the marks of plane i + 2 (last read by the update of plane i - 1)
@@ -545,7 +578,7 @@ cudaError_t launch_t(const CUtensorMap& mh, const CUtensorMap& mc, const StageAr
 
 bool supported(const AstroParams& p, const AstroGrid& g) {
     if (p.physics != ASTRO_RMHD || p.precision != ASTRO_PREC_MIXED) return false;
-    if (p.flux_mode != ASTRO_FLUX_CONSERVATIVE || p.split_stage) return false;
+    if (p.flux_mode != ASTRO_FLUX_CONSERVATIVE || !p.fused_stage) return false;
     // WENO5 / PPM: stencil radius 3 and first updated cell 3, so every tile's
     // boxes start on a 16-byte boundary (k0 - 3 = 32 t)
     if (p.recon != ASTRO_RECON_WENO && p.recon != ASTRO_RECON_PPM) return false;

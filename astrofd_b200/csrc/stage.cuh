@@ -12,6 +12,10 @@
 // and the divergence, GLM damping, resistive term and the float64 SSPRK
 // combination follow in the same thread, which writes U_k.  The reference's
 // per-cell loop (core/rmhd_core.py:1440-1557) evaluates the same faces twice.
+// The split path (per-direction face kernels + update) stays the default: on
+// B200 at 256^3 the fused kernel takes 3.85-3.93 ms per stage against the
+// split path's 3.6 ms (16 resident warps per SM, set by its 56 KB of shared
+// memory and 128 registers, against the face kernels' 32).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>

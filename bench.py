@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--graph", action="store_true",
                     help="replay CUDA graphs of one driver iteration in the timed steps "
                          "(kernel-class times then come from profiled steps after them)")
-    ap.add_argument("--stage-kernel", default="fused", choices=["fused", "split"],
+    ap.add_argument("--stage-kernel", default="split", choices=["fused", "split"],
                     help="fused: one kernel per SSPRK stage (TMA tiles, faces and update "
                          "together); split: per-direction face passes, then the update")
     ap.add_argument("--no-fp64", action="store_true", help="skip the float64 comparison arm")

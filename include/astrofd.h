@@ -74,11 +74,12 @@ typedef struct AstroParams {
     int32_t physics, recon, limiter, riemann;
     int32_t n_passive, passive_offset, resistive, flux_mode;
     int32_t precision, c2p_guess;
-    int32_t split_stage; /* 0: SSPRK stages of RMHD WENO5/PPM with HLLE or
+    int32_t fused_stage; /* 1: SSPRK stages of RMHD WENO5/PPM with HLLE or
                             "hlld", float32 faces and conservative fluxes run
-                            as one fused kernel per stage; 1: always the
-                            per-direction face passes + update (same result
-                            to float32 rounding)                           */
+                            as one fused kernel per stage (TMA-staged tiles,
+                            faces and update together); 0: the per-direction
+                            face passes + update (the default; the same
+                            result to float32 rounding)                    */
     const void* mlp;     /* device pointer to the learned-guess network's
                             parameter block (astro_mlp_param_bytes() bytes),
                             used when c2p_guess == ASTRO_GUESS_LEARNED        */
