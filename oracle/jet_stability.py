@@ -11,7 +11,8 @@ v and p caps in prim_to_cons, the hydro fallback of cons_to_prim_rmhd) is not
 stable for these relativistic jets, so a 100-step comparison of two runs of it
 measures the blow-up, not the precision of either run.
 
-usage: python oracle/jet_stability.py {oracle|reference} [n] [steps] [reference checkout]
+usage: python oracle/jet_stability.py oracle [n] [steps]
+       python oracle/jet_stability.py reference <n> <steps> <AstroFD checkout>
 """
 import json
 import math
@@ -39,7 +40,9 @@ def main():
     if which == "reference":
         os.environ["PYTHONDONTWRITEBYTECODE"] = "1"
         sys.dont_write_bytecode = True
-        sys.path.insert(0, sys.argv[4] if len(sys.argv) > 4 else "/root/reference")
+        if len(sys.argv) < 5:
+            sys.exit("reference mode needs the path of an AstroFD checkout (4th argument)")
+        sys.path.insert(0, sys.argv[4])
         from core import boundary as B, nozzle as N, rmhd_core as R
         R.configure(core)
         step = lambda a: R.step_ssprk3(a, d, d, d, dt)

@@ -272,10 +272,14 @@ def nozzle_struct(cfg):
     c.b0 = cfg.get("B0", 0.0)
     c.te = float(cfg.get("TE_NOZZLE", cfg.get("TE_AMB", 0.0)) or 0.0)
     c.ti = float(cfg.get("TI_NOZZLE", cfg.get("TI_AMB", 0.0)) or 0.0)
+    # the inflow's ionisation fractions, read only with chemistry on (the
+    # reference's settings leave them None otherwise)
     c.chemistry = 1 if cfg.get("CHEMISTRY_ENABLED", False) else 0
-    c.chem_offset = int(cfg.get("CHEM_OFFSET", 0))
-    for m, key in enumerate(("CHEM_X_HII_NOZZLE", "CHEM_X_HEII_NOZZLE", "CHEM_X_HEIII_NOZZLE")):
-        c.chem_x[m] = float(cfg.get(key, 0.0))
+    if c.chemistry:
+        c.chem_offset = int(cfg.get("CHEM_OFFSET", 0))
+        for m, key in enumerate(("CHEM_X_HII_NOZZLE", "CHEM_X_HEII_NOZZLE",
+                                 "CHEM_X_HEIII_NOZZLE")):
+            c.chem_x[m] = float(cfg.get(key, 0.0))
     nv = cfg.get("TRACER_NOZZLE_VALUES", []) or []
     av = cfg.get("TRACER_AMB_VALUES", []) or []
     for t in range(min(c.n_tracers, 8)):

@@ -405,9 +405,22 @@ def run_diagnostics(name, ref, out):
     np.savez_compressed(out, ng=np.array(ng), d=np.array(d), cfg=np.array(json.dumps(cfg)), **rec)
 
 
+def run_driver_case(name, ref, out):
+    """The reference's driver script, unchanged, on its own core modules (one
+    rank, through tests/driver_harness.py's mpi4py and json5 stand-ins)."""
+    import tempfile
+    sys.path.insert(0, os.path.dirname(HERE))
+    import driver_harness as DH
+    with tempfile.TemporaryDirectory() as tmp:
+        res = DH.run_driver(ref, name[len("driver_"):], tmp, dropin=False)
+    np.savez_compressed(out, t_end=np.array(DH.T_END), **res)
+
+
 def one(name, ref):
     out = os.path.join(HERE, name + ".npz")
-    if name in CASE_BY_NAME:
+    if name.startswith("driver_"):
+        run_driver_case(name, ref, out)
+    elif name in CASE_BY_NAME:
         run_case(name, ref, out)
     elif name.startswith("bc_"):
         run_bc(name, ref, out)
@@ -447,7 +460,10 @@ def main():
     if a.one:
         one(a.one, a.ref)
         return
-    names = a.names or ([c["name"] for c in CASES] + SPECIAL + [c["name"] for c in GR_CASES])
+    sys.path.insert(0, os.path.dirname(HERE))
+    import driver_harness as DH
+    names = a.names or ([c["name"] for c in CASES] + SPECIAL + [c["name"] for c in GR_CASES] +
+                        ["driver_" + c for c in DH.CONFIGS])
     env = dict(os.environ, PYTHONDONTWRITEBYTECODE="1", NUMBA_NUM_THREADS="1")
 
     def launch(nm):

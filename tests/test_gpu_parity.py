@@ -62,11 +62,15 @@ def test_step_fp64_vs_reference(case):
     step = m.step_ssprk3 if case["rk"] == 3 else m.step_ssprk2
     out = step(pr, *spacing(case), float(d["dt"])).cpu().numpy()
     g = d["step_out"]
+    # worst measured on B200 over the fixtures: 3.6e-9 (SRHD), 4.0e-9 (RMHD),
+    # 1.8e-8 ("hlld_full", sane cells): the con2prim solves stop at their
+    # tolerance (|f| < 1e-10 max(1, tau), 1e-12 for SRHD) after iteration
+    # counts that Numba's fastmath shifts
     if HLLD_FULL(case):
         msk = PT.sane_mask(g, case["physics"])
-        assert PT.normwise(out, g, msk) < 1e-6
+        assert PT.normwise(out, g, msk) < 5e-8
     else:
-        assert PT.normwise(out, g) < 1e-7
+        assert PT.normwise(out, g) < 1e-8
 
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
@@ -235,7 +239,7 @@ def test_rmhd_32cube_step_vs_oracle(riemann, recon):
     ref = O.step(O.params_from_config("rmhd", cfg), pr, dx, dx, dx, 0.3 * dx, 3)
     rmhd_core.configure(cfg)
     out = rmhd_core.step_ssprk3(torch.from_numpy(pr).to(DEV), dx, dx, dx, 0.3 * dx).cpu().numpy()
-    assert PT.normwise(out, ref) < 1e-7
+    assert PT.normwise(out, ref) < 1e-8
 
 
 def test_conservative_mode_conserves_mass():
