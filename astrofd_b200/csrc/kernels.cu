@@ -42,6 +42,13 @@ inline long mma_poll_limit() {
     const long long v = g_mma_poll_limit.load(std::memory_order_relaxed);
     return v > 0 ? (long)v : mlp::kPollLimit;
 }
+// Newton polish steps of the learned con2prim in the steps (test hook; -1:
+// the default of 2)
+std::atomic<int> g_step_polish{-1};
+inline int step_polish() {
+    const int v = g_step_polish.load(std::memory_order_relaxed);
+    return v >= 0 ? v : 2;
+}
 
 // Optional per-launch CUDA-event timing (astro_step_profiled, and the
 // astro_prof_start/stop sessions): an event is recorded after every launch;
@@ -708,8 +715,9 @@ __device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell) {
 }
 
 // Learned con2prim: per 128-cell tile the MLP (tcgen05, BF16, FP32 accumulate)
-// predicts (log W, log p); Z = D W + Gamma/(Gamma-1) p W^2 starts at most
-// max_polish Newton steps of the reference's update; cells that do not meet
+// predicts log(Z / (D + tau + B^2)); Newton on the reference's equation
+// continues from the better of that guess and the analytic start D + tau +
+// B^2 (r_newton_polish2) for at most max_polish steps; cells that do not meet
 // |f| < 1e-10 max(1, tau) then (or whose primitives from Z are invalid) get
 // the reference's complete con2prim, so their result is the reference's.
 // LISTED: a fallback list with a slot for every cell (fb_cap >= count);
@@ -728,7 +736,7 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     if (net) {
         if (t < 32) mlp::tmem_alloc(mlp::smem_u32(taddr_s), 64);
         if (t == 0) mlp::mbar_init_fenced(mlp::smem_u32(bar), 1);
-        mlp::load_weights(sm, a.net, true);
+        mlp::load_weights(sm, a.net);
         mlp::fence_async_smem();
         mlp::tc_fence_before();
     }
@@ -737,7 +745,6 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
     const uint32_t tmem = net ? *taddr_s : 0u;
     uint32_t phase = 0;
     const Phys<double> P = Phys<double>::from(a.p);
-    const double gfac = a.p.gamma / (a.p.gamma - 1.0);
     C2PCount cnt;
     unsigned n_cells = 0, n_polish = 0, n_fallback = 0, polish_steps = 0;
     const long ntiles = (a.count + mlp::TILE - 1) / mlp::TILE;
@@ -774,21 +781,23 @@ __global__ void __launch_bounds__(128, 5) k_c2p_learned(C2PArgs a) {
         const double B2 = U[5] * U[5] + U[6] * U[6] + U[7] * U[7];
         const double SB = U[1] * U[5] + U[2] * U[6] + U[3] * U[7];
         const double S2 = U[1] * U[1] + U[2] * U[2] + U[3] * U[3];
-        double Z;
-        if (net) {
-            // the guess only has to start Newton: float32 exponentials
-            const float logW = fmaxf(o[0] * a.net->ysd[0] + a.net->ymu[0], 0.f);
-            const float logp = o[1] * a.net->ysd[1] + a.net->ymu[1];
-            const double W = (double)__expf(fminf(logW, 20.f));
-            const double pg = (double)__expf(fmaxf(fminf(logp, 50.f), -80.f));
-            Z = rmax(D * W + gfac * pg * W * W, 1e-12);
-        } else {
-            Z = rmax(D + tau + B2, 1e-12);
-        }
+        // the analytic start D + tau + B^2 (the reference's second Newton
+        // start) and the network's Z = that start x exp(output 0)
+        const double Za = rmax(D + tau + B2, 1e-12);
+        double Z = Za;
+        bool polished;
         double q[9];
         int steps = 0;
         bool done = false;
-        if (isfinite(Z) && r_newton_polish(P, Z, a.max_polish, D, tau, B2, SB, S2, &steps)) {
+        if (net) {
+            // the guess only has to start Newton: a float32 exponential
+            const float lz = o[0] * a.net->ysd[0] + a.net->ymu[0];
+            Z = Za * (double)__expf(fmaxf(fminf(lz, 40.f), -40.f));
+            polished = isfinite(Z) && r_newton_polish2(P, Z, Za, a.max_polish, D, tau, B2, SB, S2, &steps);
+        } else {
+            polished = isfinite(Z) && r_newton_polish(P, Z, a.max_polish, D, tau, B2, SB, S2, &steps);
+        }
+        if (polished) {
             ++n_polish;
             polish_steps += steps;
             done = r_prims_from_Z_checked(P, Z, U, q);
@@ -1880,7 +1889,7 @@ static int run_stage_fused(const AstroParams* p, const AstroGrid* g, const Layou
         c.U = U; c.q = dst;
         c.count = (long)nc;
         c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
-        c.status = nullptr; c.max_polish = 2;
+        c.status = nullptr; c.max_polish = step_polish();
         c.poll_limit = mma_poll_limit();
         c.fb_count = (unsigned*)(w + L.c2pfb);
         c.fb_list = (unsigned*)(w + L.c2pfb + 256);
@@ -1918,7 +1927,7 @@ static int run_stage(const AstroParams* p, const AstroGrid* g, const Layout& L, 
         c.U = (const double*)(w + L.U); c.q = dst;
         c.count = (long)g->nx * g->ny * g->nz;
         c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
-        c.status = nullptr; c.max_polish = 2;
+        c.status = nullptr; c.max_polish = step_polish();
         c.poll_limit = mma_poll_limit();
         c.fb_count = (unsigned*)(w + L.c2pfb);
         c.fb_list = (unsigned*)(w + L.c2pfb + 256);
@@ -1976,6 +1985,12 @@ unsigned long long astro_launch_count(void) { return g_launches.load(); }
 int astro_debug_set_mma_poll_limit(long long polls) {
     if (polls < 0) return ASTRO_E_INVALID;
     g_mma_poll_limit.store(polls, std::memory_order_relaxed);
+    return ASTRO_OK;
+}
+
+int astro_debug_set_step_polish(int steps) {
+    if (steps < -1 || steps > 50) return ASTRO_E_INVALID;
+    g_step_polish.store(steps, std::memory_order_relaxed);
     return ASTRO_OK;
 }
 
@@ -2284,7 +2299,7 @@ int astro_step_gr(const AstroParams* p, const AstroGrid* g, const AstroGR* gr,
             C2PArgs c;
             c.U = U; c.q = dst; c.count = (long)nc;
             c.p = *p; c.net = (const mlp::Params*)p->mlp; c.stats = stats;
-            c.status = nullptr; c.max_polish = 2;
+            c.status = nullptr; c.max_polish = step_polish();
         c.poll_limit = mma_poll_limit();
             c.fb_count = (unsigned*)(w + L.c2pfb);
             c.fb_list = (unsigned*)(w + L.c2pfb + 256);

@@ -1,7 +1,7 @@
 // mlp.cu -- forward, backward and optimiser kernels of the learned con2prim
 // initial-guess network (see mlp.cuh for the tensor-core data layout).
 //
-//   k_mlp_forward   batched inference: raw invariants -> (log W, log p)
+//   k_mlp_forward   batched inference: raw invariants -> (log(Z / (D + tau + B^2)), log W)
 //   k_mlp_train     forward + backward of one 128-sample tile per CTA step,
 //                   gradients of the mean-squared error summed into a float32
 //                   buffer (atomics), loss summed alongside
@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const Params* P, const floa
     const int t = threadIdx.x;
     if (t < 32) tmem_alloc(smem_u32(taddr_s), 64);
     if (t == 0) mbar_init_fenced(smem_u32(bar), 1);
-    load_weights(sm, P, true);
+    load_weights(sm, P);
     fence_async_smem();
     tc_fence_before();
     __syncthreads();
@@ -197,7 +197,7 @@ __global__ void __launch_bounds__(128) k_mlp_train(const Params* P, const float*
                 }
             }
             if (l > 1) {
-                // dZ_{l-1} = dH_{l-1} * SiLU'(z_{l-1}) -> dZ buffer columns 0..63
+                // dZ_{l-1} = dH_{l-1} * ReLU'(z_{l-1}) -> dZ buffer columns 0..63
                 const int ds = l == 4 ? OFF_DS3 : (l == 3 ? OFF_DS2 : OFF_DS1);
 #pragma unroll
                 for (int cb = 0; cb < 4; ++cb) {

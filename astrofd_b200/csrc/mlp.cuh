@@ -1,8 +1,11 @@
 // mlp.cuh -- the learned con2prim initial guess: a 5 -> 64 -> 64 -> 64 -> 2
-// SiLU MLP evaluated and trained with 5th-generation tensor cores
+// ReLU MLP evaluated and trained with 5th-generation tensor cores
 // (tcgen05.mma, kind::f16, BF16 operands in shared memory, FP32 accumulators
-// in tensor memory).  No counterpart in the reference, which starts its
-// Newton iteration from a hydro fixed point (core/rmhd_core.py:255-266).
+// in tensor memory).  Outputs (normalised): log(Z / (D + tau + B^2)), the
+// Newton variable Z = rho h W^2 relative to the analytic start, and log W (an
+// auxiliary target, trained but not used by the solver).  No counterpart in
+// the reference, which starts its Newton iteration from a hydro fixed point
+// (core/rmhd_core.py:255-266).
 //
 // One CTA of 128 threads owns a tile of 128 samples: thread t <-> sample
 // (row) t <-> TMEM lane t.  Every GEMM is issued as M = 128:
@@ -47,7 +50,7 @@ constexpr int OFF_H2 = OFF_H1 + 128 * 64 * 2;
 constexpr int OFF_H3 = OFF_H2 + 128 * 64 * 2;
 constexpr int kInferSmem = OFF_H2;             // W + H0 + H1 (H1 reused per layer)
 constexpr int OFF_DZ = OFF_H3 + 128 * 64 * 2;  // [128 x 128] bf16, 32 KB (16 col groups)
-constexpr int OFF_DS1 = OFF_DZ + 128 * 128 * 2;  // SiLU'(z) of layers 1..3, bf16 16 KB each
+constexpr int OFF_DS1 = OFF_DZ + 128 * 128 * 2;  // ReLU'(z) of layers 1..3, bf16 16 KB each
 constexpr int OFF_DS2 = OFF_DS1 + 128 * 64 * 2;
 constexpr int OFF_DS3 = OFF_DS2 + 128 * 64 * 2;
 constexpr int OFF_RED = OFF_DS3 + 128 * 64 * 2;  // [128][65] f32 bias-gradient reduction
@@ -208,43 +211,23 @@ __device__ __forceinline__ void drain_after_timeout(uint32_t mbar, uint32_t phas
     mbar_wait_bounded(mbar, phase ^ 1u, nullptr);
 }
 
-// tanh.approx.f32: one MUFU operation; the PTX ISA bounds its relative error by
-// 2^-10.987, and on B200 it measures below 1e-5 over [-40, 40]
-__device__ __forceinline__ float tanh_approx(float x) {
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-// SiLU(z) = z sigmoid(z) = h (1 + tanh h), h = z/2: one MUFU operation
-// instead of an exponential and a reciprocal.  The product h (1 + tanh h)
-// cancels for large negative h, so its error is |h| times the absolute error
-// of 1 + tanh h: measured on B200 over h in [-40, 0] that error is below
-// 7.7e-6 (tanh.approx returns exactly -1 from there on), so the SiLU is within
-// 1e-5 of exact everywhere, far below the bfloat16 rounding of its output.
-__device__ __forceinline__ float silu(float z) {
-    const float h = 0.5f * z;
-    return fmaf(h, tanh_approx(h), h);
-}
-__device__ __forceinline__ float silu_grad(float z) {
-    if (z < -16.f) return 0.f;
-    const float s = fmaf(0.5f, tanh_approx(0.5f * z), 0.5f);
-    return s * (1.0f + z * (1.0f - s));
+// ReLU of two float32 values rounded to a packed bfloat16 pair (the ReLU is
+// the conversion's .relu modifier: one instruction for two columns).  The
+// first value lands in the low half, i.e. at the lower address.
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi) {
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
 }
 
-// SiLU of 16 accumulator columns after adding their biases, two columns per
-// packed float32x2 instruction (sm_100 FADD2/FFMA2).  The inference weights
-// and biases of layers 1-3 are stored halved (load_weights(.., true)): scaling
-// by 2 commutes with every rounding of the MMA and the bias add, so the sum is
-// exactly h = z/2 and SiLU(z) = h + h tanh(h) needs no multiply.
-__device__ __forceinline__ void bias_silu16(const float* z, const float* bias_half, float* h) {
+// 16 accumulator columns plus their biases -> ReLU -> 16 bfloat16 values
+// (8 packed pairs): the bias adds as packed float32x2 adds (sm_100 FADD2)
+__device__ __forceinline__ void bias_relu16(const float* z, const float* bias, uint32_t* h) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        const float2 b = *reinterpret_cast<const float2*>(bias_half + 2 * i);
-        const float2 hh = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]), b);
-        const float2 tt = make_float2(tanh_approx(hh.x), tanh_approx(hh.y));
-        const float2 ss = __ffma2_rn(hh, tt, hh);
-        h[2 * i] = ss.x;
-        h[2 * i + 1] = ss.y;
+        const float2 b = *reinterpret_cast<const float2*>(bias + 2 * i);
+        const float2 s = __fadd2_rn(make_float2(z[2 * i], z[2 * i + 1]), b);
+        h[i] = relu_bf16x2(s.x, s.y);
     }
 }
 
@@ -256,22 +239,25 @@ __device__ __forceinline__ void st_row8(unsigned char* base, int R, int r, int c
     *reinterpret_cast<uint4*>(base + elem_off(R, r, c0)) = *reinterpret_cast<uint4*>(p);
 }
 
+// the same store from 4 packed bfloat16 pairs
+__device__ __forceinline__ void st_row8_packed(unsigned char* base, int R, int r, int c0, const uint32_t* p) {
+    *reinterpret_cast<uint4*>(base + elem_off(R, r, c0)) = make_uint4(p[0], p[1], p[2], p[3]);
+}
+
 // FP32 master weights -> bf16 K-major operands in shared memory (all
-// threads).  halve: layers 1-3 and their biases at half scale (exact in bf16
-// and float32), for the inference epilogue bias_silu16.
-__device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P, bool halve = false) {
-    const float hs = halve ? 0.5f : 1.0f;
+// threads), biases in float32.
+__device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P) {
     for (int e = threadIdx.x; e < 64 * 16; e += blockDim.x) {  // W1 [64 x 16], in 5..15 = 0
         int o = e / 16, i = e % 16;
         float w = i < NIN ? P->W1[o * NIN + i] : 0.f;
-        *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W1 + elem_off(64, o, i)) = __float2bfloat16_rn(hs * w);
+        *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W1 + elem_off(64, o, i)) = __float2bfloat16_rn(w);
     }
     for (int e = threadIdx.x; e < 64 * 64; e += blockDim.x) {
         int o = e / 64, i = e % 64;
         *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W2 + elem_off(64, o, i)) =
-            __float2bfloat16_rn(hs * P->W2[o * H + i]);
+            __float2bfloat16_rn(P->W2[o * H + i]);
         *reinterpret_cast<__nv_bfloat16*>(sm + OFF_W3 + elem_off(64, o, i)) =
-            __float2bfloat16_rn(hs * P->W3[o * H + i]);
+            __float2bfloat16_rn(P->W3[o * H + i]);
     }
     for (int e = threadIdx.x; e < 16 * 64; e += blockDim.x) {  // W4 [16 x 64], rows 2..15 = 0
         int o = e / 64, i = e % 64;
@@ -280,9 +266,8 @@ __device__ __forceinline__ void load_weights(unsigned char* sm, const Params* P,
     }
     float* bs = reinterpret_cast<float*>(sm + OFF_BIAS);
     for (int e = threadIdx.x; e < 3 * H + NOUT; e += blockDim.x)
-        bs[e] = e < H ? hs * P->b1[e]
-                      : (e < 2 * H ? hs * P->b2[e - H]
-                                   : (e < 3 * H ? hs * P->b3[e - 2 * H] : P->b4[e - 3 * H]));
+        bs[e] = e < H ? P->b1[e]
+                      : (e < 2 * H ? P->b2[e - H] : (e < 3 * H ? P->b3[e - 2 * H] : P->b4[e - 3 * H]));
 }
 
 // Issue D[128 x N] (+)= A[128 x K] . B for K = 16*ksteps, both operands
@@ -298,75 +283,99 @@ __device__ __forceinline__ void mma_kmajor(uint32_t tmem_d, uint32_t a_addr, int
     }
 }
 
+// ---- the forward pass in steps, for kernels that run several tiles per
+// block or put other work between the tensor-core waits ----
+
+// H0 row `row` of the activation buffer h: 5 normalised features, zeros up
+// to 16
+__device__ __forceinline__ void store_h0(unsigned char* h, int row, const float* h0) {
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = i < NIN ? h0[i] : 0.f;
+    st_row8(h, 128, row, 0, v);
+    st_row8(h, 128, row, 8, v + 8);
+}
+
+// one thread, after a barrier preceded by fence_async_smem() and
+// tc_fence_before(): the MMAs of layer l with the activations at shared
+// address `in` (H0 for l = 0) into the accumulator columns at tmem_d,
+// committed to mbar
+__device__ __forceinline__ void issue_layer(const unsigned char* sm, uint32_t tmem_d, uint32_t mbar,
+                                            int l, uint32_t in) {
+    tc_fence_after();
+    if (l == 0) mma_kmajor(tmem_d, in, 128, smem_u32(sm + OFF_W1), 64, 64, 1);
+    else if (l < 3) mma_kmajor(tmem_d, in, 128, smem_u32(sm + (l == 1 ? OFF_W2 : OFF_W3)), 64, 64, 4);
+    else mma_kmajor(tmem_d, in, 128, smem_u32(sm + OFF_W4), 16, NOUTP, 4);
+    mma_commit(mbar);
+}
+
+// all threads of the tile, after layer l's MMAs completed (and
+// tc_fence_after): the ReLU activations of row `row` into h (l < 3), or its
+// two outputs (l == 3).  tmem_row: the accumulator columns at this thread's
+// TMEM lane.
+__device__ __forceinline__ void finish_layer(const unsigned char* sm, unsigned char* h, uint32_t tmem_row,
+                                             int row, int l, float* out) {
+    const float* bsm = reinterpret_cast<const float*>(sm + OFF_BIAS);
+    if (l < 3) {
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) {
+            float z[16];
+            uint32_t hv[8];
+            tmem_ld16(tmem_row + cb * 16, z);
+            bias_relu16(z, bsm + l * H + cb * 16, hv);
+            st_row8_packed(h, 128, row, cb * 16, hv);
+            st_row8_packed(h, 128, row, cb * 16 + 8, hv + 4);
+        }
+    } else {
+        float y[16];
+        tmem_ld16(tmem_row, y);
+        out[0] = y[0] + bsm[3 * H];
+        out[1] = y[1] + bsm[3 * H + 1];
+    }
+}
+
 // forward pass of one tile, in shared memory / TMEM.  Thread t owns row t.
 // h0: normalised features of this thread's row.  When TRAIN, keeps H1..H3 and
-// SiLU'(z) for the backward pass; otherwise H1 is reused for every layer and
-// the weights are the halved ones of load_weights(.., true).
+// ReLU'(z) for the backward pass; otherwise H1 is reused for every layer.
 // Returns false if an MMA wait timed out (uniform across the block).
 template <bool TRAIN>
 __device__ __forceinline__ bool forward_tile(unsigned char* sm, uint32_t tmem, uint32_t mbar, uint32_t& phase,
                              const Params* P, const float* h0, float* out, int* status,
                              long poll_limit = kPollLimit) {
     const int t = threadIdx.x;
-    const int warp = t >> 5;
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-    {  // H0 row: 5 features, zeros up to 16
-        float v[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = i < NIN ? h0[i] : 0.f;
-        st_row8(sm + OFF_H0, 128, t, 0, v);
-        st_row8(sm + OFF_H0, 128, t, 8, v + 8);
-    }
+    const uint32_t lane_base = (uint32_t)((t >> 5) * 32) << 16;
+    store_h0(sm + OFF_H0, t, h0);
     const float* bsm = reinterpret_cast<const float*>(sm + OFF_BIAS);
-    const int offW[3] = {OFF_W1, OFF_W2, OFF_W3};
     const int offDS[3] = {OFF_DS1, OFF_DS2, OFF_DS3};
     for (int l = 0; l < 4; ++l) {
         fence_async_smem();
         tc_fence_before();
         __syncthreads();
-        if (t == 0) {
-            tc_fence_after();
-            const int in_off = l == 0 ? OFF_H0 : (TRAIN ? OFF_H1 + (l - 1) * 128 * 64 * 2 : OFF_H1);
-            const uint32_t a = smem_u32(sm + in_off);
-            if (l < 3)
-                mma_kmajor(tmem, a, 128, smem_u32(sm + offW[l]), 64, 64, l == 0 ? 1 : 4);
-            else
-                mma_kmajor(tmem, a, 128, smem_u32(sm + OFF_W4), 16, NOUTP, 4);
-            mma_commit(mbar);
-        }
+        if (t == 0)
+            issue_layer(sm, tmem, mbar, l,
+                        smem_u32(sm + (l == 0 ? OFF_H0 : (TRAIN ? OFF_H1 + (l - 1) * 128 * 64 * 2 : OFF_H1))));
         bool ok = mbar_wait_bounded(mbar, phase, status, poll_limit);
         phase ^= 1u;
         if (!__syncthreads_and(ok)) return false;
         tc_fence_after();
-        if (l < 3) {
-            unsigned char* dst = sm + (TRAIN ? OFF_H1 + l * 128 * 64 * 2 : OFF_H1);
+        if (TRAIN && l < 3) {
+            unsigned char* dst = sm + OFF_H1 + l * 128 * 64 * 2;
 #pragma unroll
             for (int cb = 0; cb < 4; ++cb) {
-                float z[16], h[16];
+                float z[16], g[16];
+                uint32_t h[8];
                 tmem_ld16(tmem + lane_base + cb * 16, z);
-                if (TRAIN) {
+                bias_relu16(z, bsm + l * H + cb * 16, h);
+                st_row8_packed(dst, 128, t, cb * 16, h);
+                st_row8_packed(dst, 128, t, cb * 16 + 8, h + 4);
+                // ReLU'(z) = 1 where the activation is positive
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) z[i] += bsm[l * H + cb * 16 + i];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) h[i] = silu(z[i]);
-                } else {
-                    bias_silu16(z, bsm + l * H + cb * 16, h);
-                }
-                st_row8(dst, 128, t, cb * 16, h);
-                st_row8(dst, 128, t, cb * 16 + 8, h + 8);
-                if (TRAIN) {
-                    float g[16];
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) g[i] = silu_grad(z[i]);
-                    st_row8(sm + offDS[l], 128, t, cb * 16, g);
-                    st_row8(sm + offDS[l], 128, t, cb * 16 + 8, g + 8);
-                }
+                for (int i = 0; i < 16; ++i) g[i] = z[i] + bsm[l * H + cb * 16 + i] > 0.f ? 1.f : 0.f;
+                st_row8(sm + offDS[l], 128, t, cb * 16, g);
+                st_row8(sm + offDS[l], 128, t, cb * 16 + 8, g + 8);
             }
         } else {
-            float y[16];
-            tmem_ld16(tmem + lane_base, y);
-            out[0] = y[0] + bsm[3 * H];
-            out[1] = y[1] + bsm[3 * H + 1];
+            finish_layer(sm, sm + OFF_H1, tmem + lane_base, t, l, out);
         }
     }
     return true;

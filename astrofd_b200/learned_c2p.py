@@ -1,8 +1,12 @@
 """Learned con2prim initial guess: data, training and evaluation on the GPU.
 
-The network (5 -> 64 -> 64 -> 64 -> 2, SiLU) maps the invariants of a
-conserved RMHD state to (log W, log p) of the primitive state that the
-reference's full Newton con2prim (core/rmhd_core.py:249) recovers from it.
+The network (5 -> 64 -> 64 -> 64 -> 2, ReLU) maps the invariants of a
+conserved RMHD state to log(Z / (D + tau + B^2)) and log W of the primitive
+state that the reference's full Newton con2prim (core/rmhd_core.py:249)
+recovers from it: Z = rho h W^2 is the variable of the reference's Newton
+iteration and D + tau + B^2 its second starting point, so a network that
+outputs 0 reproduces that start.  log W is an auxiliary target; the solver
+uses the first output only.
 Everything runs through libastrofd_b200.so: samples are converted with the
 library's prim_to_cons, labelled with its reference con2prim, featurised, and
 the weights are trained with its tensor-core forward/backward kernels and an
@@ -123,9 +127,10 @@ def residual(U, q, gamma, p_max, v_max):
 
 
 def make_dataset(prim, engine, valid_only=False, tol=1e-8):
-    """(features [n,5], targets [n,2] = (log W, log p) of the reference
-    con2prim solution, conserved [9,n]) on the device.  valid_only keeps the
-    states whose reference solution is a root of its equation."""
+    """(features [n,5], targets [n,2] = (log(Z / (D + tau + B^2)), log W) of
+    the reference con2prim solution, conserved [9,n]) on the device.
+    valid_only keeps the states whose reference solution is a root of its
+    equation."""
     L = _lib.load()
     q = torch.as_tensor(prim, dtype=torch.float64, device="cuda").contiguous()
     U = engine.p2c_array(q)
@@ -134,7 +139,10 @@ def make_dataset(prim, engine, valid_only=False, tol=1e-8):
     X = torch.empty((n, NIN), dtype=torch.float32, device="cuda")
     _lib.check(L.astro_c2p_features(rt.ptr(U), rt.ptr(X), n, rt.stream_handle()), "features")
     v2 = (sol[1:4] ** 2).sum(0)
-    T = torch.stack([-0.5 * torch.log1p(-v2), torch.log(sol[4])], dim=1).float()
+    g = engine.p.gamma
+    Z = (sol[0] + g / (g - 1.0) * sol[4]) / (1.0 - v2)
+    Za = (U[0] + U[4] + (U[5:8] ** 2).sum(0)).clamp_min(1e-12)
+    T = torch.stack([torch.log(Z / Za), -0.5 * torch.log1p(-v2)], dim=1).float()
     ok = torch.isfinite(X).all(1) & torch.isfinite(T).all(1)
     if valid_only:
         p = engine.p

@@ -4,12 +4,13 @@
 
 Data: the learned-c2p sampler (astrofd_b200.learned_c2p.sample_primitives)
 plus cells harvested from a 128^3 magnetised-jet run of this library.  Labels:
-(log W, log p) of the reference con2prim's solution, kept only where that
+(log(Z / (D + tau + B^2)), log W) of the reference con2prim's solution, kept only where that
 solution is a root of the reference's own equation (elsewhere the reference
 returns its hydro fallback, which is no function of the inputs to learn).  Weights go to
 astrofd_b200/data/c2p_mlp.npz; a JSON report (loss, polish-step count,
-fallback rate, max relative primitive error against the full FP64 Newton,
-and the same figures without the network) is printed.
+fallback rate, the share of states converged after 0, 1 and 2 polish
+steps, max relative primitive error against the full FP64 Newton, and the
+same figures without the network) is printed.
 """
 import argparse
 import json
@@ -86,7 +87,10 @@ def main():
             q, st = LC.c2p_learned(e, Ue, params, max_polish=2)
             rel = ((q - ref).abs() / ref.abs().clamp_min(1e-300))[:5].max(dim=0).values
             n = max(st["cells"], 1)
+            hist = [LC.c2p_learned(e, Ue, params, max_polish=k)[1]["learned_polish"] / n
+                    for k in (0, 1)] + [st["learned_polish"] / n]
             out[label] = {"cells": st["cells"],
+                          "converged_within_0_1_2_polish": hist,
                           "converged_within_2_polish": st["learned_polish"] / n,
                           "fallback_rate": st["learned_fallback"] / n,
                           "mean_polish_steps": st["polish_steps"] / n,
@@ -94,7 +98,7 @@ def main():
                           "max_rel_primitive_error_vs_full_newton": float(rel.max().item()),
                           "frac_rel_error_above_1e-6": float((rel > 1e-6).float().mean().item())}
         Y = tr.forward(Xe)
-        out["guess_abs_err_logW_logp_median"] = (Y - Te).abs().median(dim=0).values.tolist()
+        out["guess_abs_err_median_logZ_logW"] = (Y - Te).abs().median(dim=0).values.tolist()
         report[name] = out
     LC.save(tr.params.cpu().numpy(), a.out, report=json.dumps(report))
     print(json.dumps(report))

@@ -509,7 +509,12 @@ KERNELS = {0: "k_face (float32 reconstruction + Riemann, one direction)",
            3: "k_c2p_learned (tcgen05 MLP guess + Newton polish)"}
 
 
-def roofline(args, prof_ms, prof_n, prec, learned):
+def _hbm_peak():
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    return float(json.load(open(pk)).get("hbm_gbs", 6650.0)) if os.path.exists(pk) else 6650.0
+
+
+def roofline(args, prof_ms, prof_n, prec, learned, sm_mhz=None):
     """Dominant kernel class of the timed steps and its achieved bandwidth in
     ALGORITHMIC bytes (the unique bytes the kernel must move) per launch."""
     peaks = {}
@@ -541,15 +546,29 @@ def roofline(args, prof_ms, prof_n, prec, learned):
         # primitives for the next stage's faces (written in 2 of 3 stages)
         units, per_unit = N ** 3, 2 * nm * 8 + (2.0 / 3.0 * nm * rs if prec == "mixed" else 0)
     achieved = units * per_unit / avg_s / 1e9
-    traffic = None
+    traffic, tdata = None, {}
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(f"{prec}:{cls}:{n}")
-    return {"bound": "hbm", "kernel": KERNELS[cls], "achieved": round(achieved, 1),
-            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic, "peak_source": which,
-            "bytes_per_launch": int(units * per_unit), "avg_launch_ms": round(avg_s * 1e3, 4),
-            "class_share": round(float(prof_ms[cls] / max(prof_ms.sum(), 1e-30)), 3)}
+        tdata = json.load(open(tf))
+        traffic = tdata.get(f"{prec}:{cls}:{n}")
+    out = {"bound": "hbm", "kernel": KERNELS[cls], "achieved": round(achieved, 1),
+           "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+           "traffic": traffic, "peak_source": which,
+           "bytes_per_launch": int(units * per_unit), "avg_launch_ms": round(avg_s * 1e3, 4),
+           "class_share": round(float(prof_ms[cls] / max(prof_ms.sum(), 1e-30)), 3)}
+    if cls == 0 and prec == "mixed" and "fp32_flop_per_face" in tdata and sm_mhz:
+        # the pipe that binds the face kernel: float32 arithmetic.  FLOP per
+        # face from ncu's instruction counters, over the float32 peak of
+        # this GPU at the clock sampled during the timed steps (128 lanes x 2
+        # FLOP per SM per clock)
+        import torch
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        flops = units * tdata["fp32_flop_per_face"] / avg_s / 1e12
+        fpk = sms * 128 * 2 * sm_mhz * 1e6 / 1e12
+        out["pipe"] = {"pipe": "fp32", "flop_per_face": tdata["fp32_flop_per_face"],
+                       "achieved": round(flops, 2), "peak": round(fpk, 1), "unit": "TFLOP/s",
+                       "frac": round(flops / fpk, 3), "clock_mhz": sm_mhz}
+    return out
 
 
 def validate_srhd(args):
@@ -657,18 +676,43 @@ def c2p_batch(args):
     ref, ms_ref = timed(lambda: e.c2p_array(U))
     out = {"config": f"c2p batch, {N} " + ("states of a 128^3 jet run" if args.c2p_jet
                                            else "sampled states"), "states": N}
+    p = e.p
+    ref_root = LC.residual(U, ref, p.gamma, p.p_max, p.v_max) < 1e-8
     for name, prm in (("learned", params), ("analytic_start", None)):
         (q, st), ms = timed(lambda: LC.c2p_learned(e, U, prm, max_polish=2))
         rel = ((q[:5] - ref[:5]).abs() / ref[:5].abs().clamp_min(1e-300)).amax(0)
         n = st["cells"]
+        # states off the reference's result: where both results solve the
+        # reference's equation (other roots of f(Z) when v.B != 0), where only
+        # this path found a root (the reference fell back to its hydro
+        # solve), and misses (this path's result is no root)
+        off = rel > 1e-6
+        root = LC.residual(U, q, p.gamma, p.p_max, p.v_max) < 1e-8
+        miss = off & ~root
+        within = [LC.c2p_learned(e, U, prm, max_polish=k)[1]["learned_polish"] / n
+                  for k in (0, 1)] + [st["learned_polish"] / n]
         out[name] = {"states_per_s": N / (ms / 1e3), "ms": ms,
-                     "newton_steps_per_polished_state": st["polish_steps"] / max(n, 1),
+                     "newton_steps_per_state": st["polish_steps"] / max(n, 1),
+                     "polished_within_0_1_2": within,
+                     "polish_step_histogram": {"0": within[0], "1": within[1] - within[0],
+                                               "2": within[2] - within[1],
+                                               "fallback": st["learned_fallback"] / n},
                      "polished_within_2": st["learned_polish"] / n,
                      "fallback_rate": st["learned_fallback"] / n,
-                     "max_rel_err": float(rel.max()),
+                     "off_reference": {"other_root": float((off & root & ref_root).double().mean()),
+                                       "root_where_reference_fell_back":
+                                           float((off & root & ~ref_root).double().mean()),
+                                       "miss": float(miss.double().mean())},
+                     "max_rel_err_misses": float(rel[miss].max()) if bool(miss.any()) else 0.0,
+                     "max_rel_err_all": float(rel.max()),
                      "p999_rel_err": float(torch.quantile(rel[::max(1, N // 1000000)].float(), 0.999)),
-                     "frac_rel_err_gt_1e-6": float((rel > 1e-6).double().mean()),
+                     "frac_rel_err_gt_1e-6": float(off.double().mean()),
                      "status": st["status"]}
+        # release this arm's arrays before the next arm's timed calls, so that
+        # those do not wait on the allocator freeing cached blocks
+        del q, rel, off, root, miss
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
     out["reference_c2p"] = {"states_per_s": N / (ms_ref / 1e3), "ms": ms_ref}
     print(json.dumps(out), flush=True)
 
@@ -857,7 +901,15 @@ def main():
         "gpu_launches": mixed["launches"],
         "launch_mode": mixed["launch_mode"],
         "clocks": mixed["clocks"],
-        "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed", learned),
+        "roofline": roofline(args, mixed["prof_ms"], mixed["prof_n"], "mixed", learned,
+                             (mixed["clocks"] or {}).get("sm_mhz")),
+        # the whole step against the minimum unique HBM bytes of an SSPRK3
+        # step with 11 float64 variables: 1056 B per zone update (read the
+        # step input and the stage states, write U and the primitives)
+        "step_roofline": {"bytes_per_zone_update": 1056,
+                          "achieved": round(n ** 3 * 1056 / (mixed["ms"] / args.steps / 1e3) / 1e9, 1),
+                          "unit": "GB/s", "frac": round(n ** 3 * 1056 / (mixed["ms"] / args.steps / 1e3)
+                                                        / 1e9 / _hbm_peak(), 4)},
         "kernel_ms_per_step": {k: round(mixed["prof_ms"][c] / mixed["prof_steps"], 3)
                                for k, c in (("face", 0), ("update", 1), ("c2p_learned", 3),
                                             ("c2p_fallback", 4), ("other", 2))},

@@ -20,8 +20,9 @@
  *   - Thread safety: calls on different streams are independent, with two
  *     exceptions that share process-wide state: astro_rhs_static, whose
  *     scratch is one array in the library's device memory shared by every
- *     call on a device, and the astro_prof_start/stop and
- *     astro_debug_set_mma_poll_limit settings.
+ *     call on a device, and the astro_prof_start/stop,
+ *     astro_debug_set_mma_poll_limit and astro_debug_set_step_polish
+ *     settings.
  */
 #ifndef ASTROFD_B200_H
 #define ASTROFD_B200_H
@@ -128,9 +129,10 @@ typedef struct AstroC2PStats {
                                           a learned-guess block whose tensor-core
                                           wait ran out finishes its cells from
                                           Z = D + tau + B^2 (the result is still the
-                                          full solve's); a fused stage block whose
-                                          tile load never landed leaves its cells
-                                          unupdated (the step's result is invalid) */
+                                          full solve's); a learned-guess or fused
+                                          stage block whose bulk/tile load never
+                                          landed leaves its cells unsolved (the
+                                          call's result is invalid) */
 } AstroC2PStats;
 
 /* --- build / diagnostics ------------------------------------------------ */
@@ -220,6 +222,12 @@ unsigned long long astro_launch_count(void);
  * the kernels then finish without the network and wait for those MMAs
  * before freeing their tensor memory. */
 int astro_debug_set_mma_poll_limit(long long polls);
+/* Test hook, no counterpart in the reference: Newton polish steps the
+ * learned con2prim of astro_step / astro_step_stage / astro_step_gr allows
+ * before a cell goes to the reference's complete solve, for the calls that
+ * follow (-1 restores the default of 2; 0 sends every cell whose start does
+ * not already meet the tolerance to that solve). */
+int astro_debug_set_step_polish(int steps);
 /* No reference counterpart: kernel-class times over any sequence of this
  * library's calls, without host synchronisation in between.
  * astro_prof_start records an event on `stream`, then one after each of the
@@ -267,13 +275,15 @@ int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t co
               AstroC2PStats* stats, void* stream);
 
 /* --- learned con2prim initial guess (no counterpart in the reference) ------
- * A 5-64-64-64-2 SiLU network on the invariants (log D, log1p|S|/D,
- * log1p tau/D, log1p B^2/D, log1p (S.B)^2/D^3) predicts (log W, log p); the
- * resulting Z = D W + Gamma/(Gamma-1) p W^2 starts at most max_polish Newton
- * steps of the reference's update (core/rmhd_core.py:268-292).  Cells whose
- * residual is still >= 1e-10 max(1, tau) continue with the full Newton solve
- * and then, if needed, the reference's complete con2prim.  Evaluation and
- * training use tcgen05 tensor cores (BF16 operands, FP32 accumulation).
+ * A 5-64-64-64-2 ReLU network on the invariants (log D, log1p|S|/D,
+ * log1p tau/D, log1p B^2/D, log1p (S.B)^2/D^3) predicts log(Z / (D + tau +
+ * B^2)) of the solution's Z = rho h W^2 (and log W, a training target only).
+ * At most max_polish Newton steps of the reference's update
+ * (core/rmhd_core.py:268-292) follow, from whichever of the network's Z and
+ * the reference's second start D + tau + B^2 has the shorter first step.
+ * Cells whose residual is then still >= 1e-10 max(1, tau) get the reference's
+ * complete con2prim.  Evaluation and training use tcgen05 tensor cores (BF16
+ * operands, FP32 accumulation).
  * The parameter block is float32: W1[64x5] b1[64] W2[64x64] b2[64] W3[64x64]
  * b3[64] W4[2x64] b4[2] (the astro_mlp_trainable() trainable floats), then
  * xmu[5] xsd[5] ymu[2] ysd[2] (feature / target normalisation).  `status`
