@@ -716,8 +716,9 @@ __device__ __forceinline__ bool c2p_defer(const C2PArgs& a, long cell) {
 
 // Learned con2prim: per 128-cell tile the MLP (tcgen05, BF16, FP32 accumulate)
 // predicts log(Z / (D + tau + B^2)); Newton on the reference's equation
-// continues from the better of that guess and the analytic start D + tau +
-// B^2 (r_newton_polish2) for at most max_polish steps; cells that do not meet
+// continues from that guess or, where its first step is not already short,
+// from the better of it and the analytic start D + tau + B^2
+// (r_newton_polish2), for at most max_polish steps; cells that do not meet
 // |f| < 1e-10 max(1, tau) then (or whose primitives from Z are invalid) get
 // the reference's complete con2prim, so their result is the reference's.
 // LISTED: a fallback list with a slot for every cell (fb_cap >= count);

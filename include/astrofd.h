@@ -279,8 +279,9 @@ int astro_c2p(const AstroParams* p, const double* cons, double* prim, int64_t co
  * log1p tau/D, log1p B^2/D, log1p (S.B)^2/D^3) predicts log(Z / (D + tau +
  * B^2)) of the solution's Z = rho h W^2 (and log W, a training target only).
  * At most max_polish Newton steps of the reference's update
- * (core/rmhd_core.py:268-292) follow, from whichever of the network's Z and
- * the reference's second start D + tau + B^2 has the shorter first step.
+ * (core/rmhd_core.py:268-292) follow, from the network's Z or, where its
+ * first step exceeds 1e-2 Z, from whichever of it and the reference's second
+ * start D + tau + B^2 has the shorter first step.
  * Cells whose residual is then still >= 1e-10 max(1, tau) get the reference's
  * complete con2prim.  Evaluation and training use tcgen05 tensor cores (BF16
  * operands, FP32 accumulation).
