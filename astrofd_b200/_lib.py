@@ -109,6 +109,7 @@ PROTOS = {
     "astro_launch_count": (C.c_ulonglong, []),
     "astro_debug_set_mma_poll_limit": (C.c_int, [C.c_longlong]),
     "astro_debug_set_step_polish": (C.c_int, [C.c_int]),
+    "astro_debug_set_tile_poll_limit": (C.c_int, [C.c_longlong]),
     "astro_max_char_speed_workspace_bytes": (C.c_size_t, []),
     "astro_max_char_speed": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP,
                                        _DP, _VP, C.c_size_t, _VP]),

@@ -42,6 +42,12 @@ inline long mma_poll_limit() {
     const long long v = g_mma_poll_limit.load(std::memory_order_relaxed);
     return v > 0 ? (long)v : mlp::kPollLimit;
 }
+// polls per tile-load wait of the fused stage kernel (test hook)
+std::atomic<long long> g_tile_poll_limit{0};
+inline long tile_poll_limit() {
+    const long long v = g_tile_poll_limit.load(std::memory_order_relaxed);
+    return v > 0 ? (long)v : astro_stage::kTilePollLimit;
+}
 // Newton polish steps of the learned con2prim in the steps (test hook; -1:
 // the default of 2)
 std::atomic<int> g_step_polish{-1};
@@ -1875,6 +1881,7 @@ static int run_stage_fused(const AstroParams* p, const AstroGrid* g, const Layou
     a.lo = b.lo; a.hi[0] = b.hi[0]; a.hi[1] = b.hi[1]; a.hi[2] = b.hi[2];
     a.dd[0] = g->dx; a.dd[1] = g->dy; a.dd[2] = g->dz; a.dt = dt;
     a.stage = st; a.nstages = nst; a.p = *p;
+    a.poll_limit = tile_poll_limit();
     cudaError_t e = astro_stage::launch(a, s);
     if (e != cudaSuccess) return ASTRO_E_CUDA;
     mark(0, s);
@@ -1986,6 +1993,12 @@ unsigned long long astro_launch_count(void) { return g_launches.load(); }
 int astro_debug_set_mma_poll_limit(long long polls) {
     if (polls < 0) return ASTRO_E_INVALID;
     g_mma_poll_limit.store(polls, std::memory_order_relaxed);
+    return ASTRO_OK;
+}
+
+int astro_debug_set_tile_poll_limit(long long polls) {
+    if (polls < 0) return ASTRO_E_INVALID;
+    g_tile_poll_limit.store(polls, std::memory_order_relaxed);
     return ASTRO_OK;
 }
 

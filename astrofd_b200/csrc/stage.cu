@@ -62,7 +62,7 @@ constexpr int OFF_FAIL = OFF_CNT + 4 * (NRING + 1);
 constexpr int kSmem = OFF_FAIL + 4 * 3 * kJobs;
 static_assert(OFF_RING % 128 == 0 && CORE_STRIDE * 4 % 128 == 0, "TMA alignment");
 static_assert(kSmem <= 56 * 1024, "four blocks per SM");
-constexpr long kPollLimit = 1L << 24;  // polls of a tile-load wait before it gives up
+constexpr long kPollLimit = kTilePollLimit;  // polls of a tile-load wait before it gives up
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -85,9 +85,27 @@ __device__ __forceinline__ bool bar_try(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait; false if the load did not land within the poll budget
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
-    for (long it = 0; it < kPollLimit; ++it)
+__device__ __forceinline__ bool bar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait; false if the load did not land within `limit` polls.  A
+// limit of a few polls (a test setting) uses non-blocking probes, since one
+// try_wait may itself suspend the thread until the phase completes.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, long limit = kPollLimit) {
+    if (limit < 1024) {
+        for (long it = 0; it < limit; ++it)
+            if (bar_test(bar, parity)) return true;
+        return false;
+    }
+    for (long it = 0; it < limit; ++it)
         if (bar_try(bar, parity)) return true;
     return false;
 }
@@ -319,7 +337,8 @@ __global__ void __launch_bounds__(kThreads, 4)
         for (int pl = i0 - 3; pl <= i0 + 2; ++pl) load_ring(pl);
     // planes i0-3 .. i0+1 here; the loop's first pass waits for i0+2
     bool w0 = true;
-    for (int pl = i0 - 3; pl <= i0 + 1; ++pl) w0 &= bar_wait(bar0 + 8 * slot_of(pl), parity_of(pl));
+    for (int pl = i0 - 3; pl <= i0 + 1; ++pl)
+        w0 &= bar_wait(bar0 + 8 * slot_of(pl), parity_of(pl), a.poll_limit);
     bool ok = __syncthreads_and(w0);
 
     float Flo[NM], Fhi[NM];
@@ -350,8 +369,8 @@ __global__ void __launch_bounds__(kThreads, 4)
                     asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + (size_t)v * nc + cell));
             }
         }
-        bool w = bar_wait(bar0 + 8 * slot_of(i + 3), parity_of(i + 3));
-        if (cells) w &= bar_wait(hbar, (uint32_t)((i - i0) & 1));
+        bool w = bar_wait(bar0 + 8 * slot_of(i + 3), parity_of(i + 3), a.poll_limit);
+        if (cells) w &= bar_wait(hbar, (uint32_t)((i - i0) & 1), a.poll_limit);
         ok = __syncthreads_and(w);
         if (!ok) break;
         // jobs: y and z faces warp-strided (none for plane i0 - 1), then the
@@ -467,8 +486,9 @@ __global__ void __launch_bounds__(kThreads, 4)
     }
     if (!ok) {
         // a tile load did not land in time: before the block's shared memory
-        // goes away, wait (bounded again) for the last load issued on every
-        // barrier (at most one per barrier is ever outstanding), and report
+        // goes away, wait (bounded again, with the full budget whatever the
+        // tile waits had) for the last load issued on every barrier (at most
+        // one per barrier is ever outstanding), and report
         if (t == 0) {
             for (int s = 0; s <= NRING; ++s)
                 if (issued[s] > 0) bar_wait(bar0 + 8 * s, (issued[s] - 1) & 1u);

@@ -43,8 +43,11 @@ struct StageArgs {
     int lo, hi[3];        // updated cells [lo, hi[d]) per direction
     double dd[3], dt;
     int stage, nstages;
+    long poll_limit;      // polls per tile-load wait (the default, or a test setting)
     AstroParams p;
 };
+// polls per tile-load wait unless a test sets fewer
+constexpr long kTilePollLimit = 1L << 24;
 
 // whether the fused kernel covers this configuration: RMHD, float32 faces,
 // conservative fluxes, WENO5 or PPM, HLLE or "hlld", no passive fluxes

@@ -21,8 +21,8 @@
  *     exceptions that share process-wide state: astro_rhs_static, whose
  *     scratch is one array in the library's device memory shared by every
  *     call on a device, and the astro_prof_start/stop,
- *     astro_debug_set_mma_poll_limit and astro_debug_set_step_polish
- *     settings.
+ *     astro_debug_set_mma_poll_limit, astro_debug_set_tile_poll_limit and
+ *     astro_debug_set_step_polish settings.
  */
 #ifndef ASTROFD_B200_H
 #define ASTROFD_B200_H
@@ -222,6 +222,13 @@ unsigned long long astro_launch_count(void);
  * the kernels then finish without the network and wait for those MMAs
  * before freeing their tensor memory. */
 int astro_debug_set_mma_poll_limit(long long polls);
+/* Test hook, no counterpart in the reference: polls each tile-load wait of
+ * the fused stage kernel (AstroParams.fused_stage) makes before giving up,
+ * for the launches that follow (0 restores the default of 2^24).  A block
+ * whose wait gives up stops, waits with the full budget for its loads still
+ * in flight, and counts itself in AstroC2PStats.wait_timeouts; its cells are
+ * not updated, so that step's result is invalid. */
+int astro_debug_set_tile_poll_limit(long long polls);
 /* Test hook, no counterpart in the reference: Newton polish steps the
  * learned con2prim of astro_step / astro_step_stage / astro_step_gr allows
  * before a cell goes to the reference's complete solve, for the calls that

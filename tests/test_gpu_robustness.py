@@ -10,6 +10,8 @@ the C ABI on the device.
   thread block finishes its cells from the analytic start, waits for the MMAs
   still in flight before freeing its tensor memory, and the step counts the
   event in AstroC2PStats.wait_timeouts; the primitives are the full solve's.
+* A tile-load wait of the fused stage kernel that gives up: the block waits
+  for its loads still in flight, stops and is counted in wait_timeouts.
 """
 import ctypes as C
 
@@ -109,3 +111,45 @@ def test_learned_con2prim_recovers_from_a_wait_that_gives_up(precision):
     again, st_again = step("learned")
     assert st_again["wait_timeouts"] == 0
     assert PT.normwise(again, normal) == 0.0
+
+
+def test_fused_stage_reports_a_tile_wait_that_gives_up():
+    """The fused stage kernel's tile-load waits are bounded.  With a budget of
+    one non-blocking poll (astro_debug_set_tile_poll_limit(1)) they give up
+    while the TMA loads are still in flight: every block then waits for its
+    loads with the full budget before its shared memory goes away, stops, and
+    counts itself in AstroC2PStats.wait_timeouts, so the caller learns that
+    the step's result is invalid.  The device stays usable: the next step,
+    with the default budget, equals a normal fused step bit for bit."""
+    L = _lib.load()
+    N, NG = 32, 3
+    core, noz, _ = rmhd_jet_config(N, NG)
+    d = 1.0 / N
+    base = torch.from_numpy(rmhd_jet(N, NG)).cuda()
+    boundary.apply_periodic_yz(base, NG)
+    boundary.apply_outflow_right_x(base, NG)
+    nozzle.apply_nozzle_left_x(base, d, d, d, N, N, 0.5, 0.5, np.random.default_rng(7), noz)
+    rmhd_core.configure(dict(core, PRECISION="mixed", FLUX_MODE="conservative",
+                             C2P_GUESS="reference", STAGE_KERNEL="fused"))
+
+    def step():
+        rmhd_core.c2p_stats(reset=True)
+        out = rmhd_core.step_ssprk3(base.clone(), d, d, d, core["CFL"] * d)
+        torch.cuda.synchronize()
+        return out.cpu().numpy(), rmhd_core.c2p_stats(reset=True)
+
+    try:
+        normal, st_normal = step()
+        assert st_normal["wait_timeouts"] == 0
+        assert np.isfinite(normal).all()
+        assert L.astro_debug_set_tile_poll_limit(1) == 0
+        try:
+            _, st = step()
+        finally:
+            assert L.astro_debug_set_tile_poll_limit(0) == 0
+        assert st["wait_timeouts"] > 0, st
+        again, st_again = step()
+        assert st_again["wait_timeouts"] == 0
+        assert np.array_equal(again, normal)
+    finally:
+        rmhd_core.configure(dict(core, STAGE_KERNEL="split"))
