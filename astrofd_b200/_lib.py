@@ -110,6 +110,7 @@ PROTOS = {
     "astro_debug_set_mma_poll_limit": (C.c_int, [C.c_longlong]),
     "astro_debug_set_step_polish": (C.c_int, [C.c_int]),
     "astro_debug_set_tile_poll_limit": (C.c_int, [C.c_longlong]),
+    "astro_debug_rcp_f64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "astro_max_char_speed_workspace_bytes": (C.c_size_t, []),
     "astro_max_char_speed": (C.c_int, [C.POINTER(AstroParams), C.POINTER(AstroGrid), _DP,
                                        _DP, _VP, C.c_size_t, _VP]),

@@ -879,6 +879,12 @@ __global__ void k_c2p_features(const double* U, float* x, long count) {
     }
 }
 
+// the learned polish's float64 reciprocal over an array (test hook)
+__global__ void k_rcp_f64(const double* x, double* y, long n) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        y[i] = rcp_nr(x[i]);
+}
+
 int g_sm_count = 0;
 int sm_count_cached() {
     if (!g_sm_count) {
@@ -1994,6 +2000,15 @@ int astro_debug_set_mma_poll_limit(long long polls) {
     if (polls < 0) return ASTRO_E_INVALID;
     g_mma_poll_limit.store(polls, std::memory_order_relaxed);
     return ASTRO_OK;
+}
+
+int astro_debug_rcp_f64(const double* x, double* y, int64_t n, void* stream) {
+    if (n < 0) return ASTRO_E_INVALID;
+    if (n == 0) return ASTRO_OK;
+    if (!x || !y) return ASTRO_E_INVALID;
+    const int grid = (int)((n + 255) / 256 < 65535 ? (n + 255) / 256 : 65535);
+    k_rcp_f64<<<grid, 256, 0, (cudaStream_t)stream>>>(x, y, (long)n);
+    return cudaGetLastError() == cudaSuccess ? ASTRO_OK : ASTRO_E_CUDA;
 }
 
 int astro_debug_set_tile_poll_limit(long long polls) {

@@ -58,6 +58,26 @@ template <typename R> AHD R rsq_(R x) {
 #endif
     return R(1) / sqrt(x);
 }
+// Float64 reciprocal for the learned con2prim's polish (not the reference's
+// own solve, which keeps IEEE divisions): the hardware approximation
+// rcp.approx.ftz.f64 refined by two Newton-Raphson steps for 1/x,
+// r <- r + r (1 - x r), each of which squares the relative error, which ends
+// at float64 rounding (within 2 ulp of 1/x, checked on the device against the
+// IEEE quotient).  For normal, non-zero x, which is all its callers pass; a
+// subnormal x is flushed to zero.
+AHD double rcp_nr(double x) {
+#ifdef __CUDA_ARCH__
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+#else
+    return 1.0 / x;
+#endif
+}
+
 // a / b: float32 as a * rcp(b), float64 as the IEEE quotient
 template <typename R> AHD R qdiv(R a, R b) {
     if constexpr (sizeof(R) == 4) return a * rcp_(b);
@@ -883,9 +903,11 @@ AHD void r_c2p_start(const Phys<double>& P, const double* U, double* q0, double&
 // clamped quantity is constant and contributes nothing.
 AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, double B2,
                        double SB, double S2, double* df, double tol) {
-    // the reference's divisions regrouped around four quotients (1/Z,
-    // 1/(Z+B^2)^2, 1/(1-v^2), Z/(rho W^2)) and one square root: the same
-    // residual to rounding, far inside the Newton tolerance
+    // the reference's divisions regrouped: one division (1/Z and
+    // 1/(Z+B^2)^2 from their product), one reciprocal square root (W), and
+    // p = (G-1)/G (Z / W^2 - rho), the reference's (h - 1) rho (G-1)/G with
+    // h = Z / (rho W^2) written without a quotient: the same residual to
+    // rounding, far inside the Newton tolerance
     const double G = P.gamma, SM = 1e-12;
     const double Zf = rmax(Z, SM);
     const double ZpB = Z + B2;
@@ -895,7 +917,7 @@ AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, do
     double iZ, iBq;
     const double ZB = Zf * Bq;
     if (ZB < 1e300) {
-        const double t = 1.0 / ZB;
+        const double t = rcp_nr(ZB);
         iZ = t * Bq;
         iBq = t * Zf;
     } else {
@@ -911,9 +933,9 @@ AHD double r_f_df_of_Z(const Phys<double>& P, double Z, double D, double tau, do
     const double W = rsqrt(om);
     const double W2 = W * W;
     const double rho = D * (om * W);  // D / W, W >= 1
-    const double h = Z / rmax(D * W, SM);  // rho W^2 = D W
     const double gm = (G - 1.0) / G;
-    double p = (h - 1.0) * rho * gm;
+    // (h - 1) rho with h = Z / (rho W^2) is Z / W^2 - rho: no division
+    double p = (Z * om - rho) * gm;
     bool pcap = false;
     if (p < SM) { p = SM; pcap = true; }
     if (p > P.p_max) { p = P.p_max; pcap = true; }
@@ -955,7 +977,7 @@ AHD bool r_newton_polish(const Phys<double>& P, double& Z, int max_steps, double
         }
         if (s == max_steps) break;
         if (dfdZ == 0.0 || !isfinite(dfdZ)) break;
-        double dZ = -f / dfdZ;
+        double dZ = -f * rcp_nr(dfdZ);
         if (dZ > 0.5 * Z) dZ = 0.5 * Z;
         if (dZ < -0.5 * Z) dZ = -0.5 * Z;
         Z += dZ;
@@ -998,7 +1020,7 @@ AHD bool r_newton_polish2(const Phys<double>& P, double& Z, double Zb, int max_s
     }
     for (int s = 1; s <= max_steps; ++s) {
         if (df == 0.0 || !isfinite(df)) break;
-        double dZ = -f / df;
+        double dZ = -f * rcp_nr(df);
         if (dZ > 0.5 * Z) dZ = 0.5 * Z;
         if (dZ < -0.5 * Z) dZ = -0.5 * Z;
         Z += dZ;
@@ -1028,7 +1050,7 @@ AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U
     const double Zf = rmax(Z, SM), ZBf = rmax(ZpB, SM);
     double iZ, iZB;
     if (Zf * ZBf < 1e300) {
-        const double t = 1.0 / (Zf * ZBf);
+        const double t = rcp_nr(Zf * ZBf);
         iZ = t * ZBf;
         iZB = t * Zf;
     } else {
@@ -1048,8 +1070,8 @@ AHD bool r_prims_from_Z_checked(const Phys<double>& P, double Z, const double* U
     const double om = 1.0 - (vx * vx + vy * vy + vz * vz);  // 1 / W^2
     const double W = rsqrt(om);
     double rho = D * (om * W);                               // D / W, W >= 1
-    double h = Z / rmax(D * W, SM);                          // rho / om = D W
-    double p = (h - 1.0) * rho * ((G - 1.0) / G);
+    // (h - 1) rho with h = Z / (rho W^2) is Z / W^2 - rho: no division
+    double p = (Z * om - rho) * ((G - 1.0) / G);
     if (!isfinite(rho) || !isfinite(p) || rho <= 0.0 || p <= 0.0) return false;
     q[0] = rho; q[1] = vx; q[2] = vy; q[3] = vz; q[4] = p;
     q[5] = Bx; q[6] = By; q[7] = Bz; q[8] = U[8];

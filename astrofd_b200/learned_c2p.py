@@ -212,15 +212,17 @@ class Trainer:
         return Y
 
 
-def c2p_learned(engine, U, params, max_polish=2, listed=True):
+def c2p_learned(engine, U, params, max_polish=2, listed=True, out=None):
     """Batch con2prim with the learned guess (params=None: Z = D + tau + B^2
     start).  listed: solve the states whose polish fails in a second kernel
-    (else inline).  Returns (primitives [9,n], stats dict)."""
+    (else inline).  out: an optional preallocated [9,n] result.  Returns
+    (primitives [9,n], stats dict)."""
     L = _lib.load()
     p = _lib.AstroParams()
     C.memmove(C.byref(p), C.byref(engine.p), C.sizeof(p))
     p.mlp = None if params is None else params.data_ptr()
-    out = torch.empty_like(U)
+    if out is None:
+        out = torch.empty_like(U)
     stats = torch.zeros(8, dtype=torch.int64, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     nb = L.astro_c2p_learned_workspace_bytes(U.shape[1]) if listed else 0

@@ -662,6 +662,10 @@ def c2p_batch(args):
     N = U.shape[1]
     params = torch.as_tensor(LC.load(args.c2p_net or LC.DATA), dtype=torch.float32).cuda()
 
+    # one result buffer for every timed call, so that no call waits on the
+    # caching allocator for a fresh 1.2 GB block
+    qbuf = torch.empty_like(U)
+
     def timed(fn, reps=3):
         fn()
         torch.cuda.synchronize()
@@ -679,7 +683,8 @@ def c2p_batch(args):
     p = e.p
     ref_root = LC.residual(U, ref, p.gamma, p.p_max, p.v_max) < 1e-8
     for name, prm in (("learned", params), ("analytic_start", None)):
-        (q, st), ms = timed(lambda: LC.c2p_learned(e, U, prm, max_polish=2))
+        torch.cuda.empty_cache()
+        (q, st), ms = timed(lambda: LC.c2p_learned(e, U, prm, max_polish=2, out=qbuf))
         rel = ((q[:5] - ref[:5]).abs() / ref[:5].abs().clamp_min(1e-300)).amax(0)
         n = st["cells"]
         # states off the reference's result: where both results solve the

@@ -229,6 +229,11 @@ int astro_debug_set_mma_poll_limit(long long polls);
  * in flight, and counts itself in AstroC2PStats.wait_timeouts; its cells are
  * not updated, so that step's result is invalid. */
 int astro_debug_set_tile_poll_limit(long long polls);
+/* Test hook, no counterpart in the reference: y[i] = the float64 reciprocal
+ * of x[i] that the learned con2prim's polish uses in place of IEEE division
+ * (a hardware approximation refined by two Newton-Raphson steps), so a test
+ * can check its error bound against the IEEE quotient.  Device arrays. */
+int astro_debug_rcp_f64(const double* x, double* y, int64_t n, void* stream);
 /* Test hook, no counterpart in the reference: Newton polish steps the
  * learned con2prim of astro_step / astro_step_stage / astro_step_gr allows
  * before a cell goes to the reference's complete solve, for the calls that
