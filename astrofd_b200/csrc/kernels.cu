@@ -416,6 +416,9 @@ struct UpdArgs {
     int nv, nx, ny, nz;
     Bounds b;
     double dd[3], dt;
+    // 1/dd and 1/(dd^2 + 1e-12), the IEEE quotients the kernel would form
+    // per cell, computed once on the host (the same values)
+    double idd[3], idd2[3];
     int stage, nstages, rhs_only;
     int defer_c2p;       // learned con2prim: write U every stage, primitives later
     int frame_only;      // only the cells outside the updated range (the fused
@@ -510,7 +513,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 8) k_update(UpdArg
             if constexpr (sizeof(RF) == 4) {
                 // float32 fluxes: multiply by 1/dx (the float64 path divides
                 // as the reference does)
-                const double i0 = 1.0 / a.dd[0], i1 = 1.0 / a.dd[1], i2 = 1.0 / a.dd[2];
+                const double i0 = a.idd[0], i1 = a.idd[1], i2 = a.idd[2];
 #pragma unroll
                 for (int v = 0; v < NM; ++v) {
                     double r = 0.0;
@@ -534,9 +537,7 @@ __global__ void __launch_bounds__(kUpdateBlock, PASSIVE ? 1 : 8) k_update(UpdArg
                 const double psi = q[8 * nc + cell];
                 rhs[8] -= a.p.glm_cp * a.p.glm_cp * psi;
                 for (int rep = 0; rep < nres; ++rep) {
-                    const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
-                    const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
-                    const double iz2 = 1.0 / (a.dd[2] * a.dd[2] + 1e-12);
+                    const double ix2 = a.idd2[0], iy2 = a.idd2[1], iz2 = a.idd2[2];
 #pragma unroll
                     for (int c = 5; c < 8; ++c) {
                         const double* B = q + (size_t)c * nc + cell;
@@ -1130,6 +1131,10 @@ UpdArgs update_args(const AstroParams& p, const AstroGrid& g, const Bounds& b, c
     u.nv = g.nv; u.nx = g.nx; u.ny = g.ny; u.nz = g.nz;
     u.b = b;
     u.dd[0] = g.dx; u.dd[1] = g.dy; u.dd[2] = g.dz;
+    for (int d = 0; d < 3; ++d) {
+        u.idd[d] = 1.0 / u.dd[d];
+        u.idd2[d] = 1.0 / (u.dd[d] * u.dd[d] + 1e-12);
+    }
     u.p = p;
     return u;
 }
