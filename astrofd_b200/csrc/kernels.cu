@@ -1891,6 +1891,10 @@ static int run_stage_fused(const AstroParams* p, const AstroGrid* g, const Layou
     a.nv = g->nv; a.nx = g->nx; a.ny = g->ny; a.nz = g->nz; a.pitch = L.pitch;
     a.lo = b.lo; a.hi[0] = b.hi[0]; a.hi[1] = b.hi[1]; a.hi[2] = b.hi[2];
     a.dd[0] = g->dx; a.dd[1] = g->dy; a.dd[2] = g->dz; a.dt = dt;
+    for (int d = 0; d < 3; ++d) {
+        a.idd[d] = 1.0 / a.dd[d];
+        a.idd2[d] = 1.0 / (a.dd[d] * a.dd[d] + 1e-12);
+    }
     a.stage = st; a.nstages = nst; a.p = *p;
     a.poll_limit = tile_poll_limit();
     cudaError_t e = astro_stage::launch(a, s);

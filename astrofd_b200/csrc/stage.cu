@@ -196,7 +196,7 @@ __device__ __forceinline__ void update_cell(const StageArgs& a, int i, int j, in
                                             const double* lap = nullptr) {
     const size_t nc = (size_t)a.nx * a.ny * a.nz;
     const size_t cell = ((size_t)i * a.ny + j) * a.nz + k;
-    const double i0d = 1.0 / a.dd[0], i1d = 1.0 / a.dd[1], i2d = 1.0 / a.dd[2];
+    const double i0d = a.idd[0], i1d = a.idd[1], i2d = a.idd[2];
     double rhs[NM];
 #pragma unroll
     for (int v = 0; v < NM; ++v) {
@@ -213,9 +213,7 @@ __device__ __forceinline__ void update_cell(const StageArgs& a, int i, int j, in
         for (int c = 0; c < 3; ++c) rhs[5 + c] += a.p.resistivity * lap[c];
     } else if (a.p.resistive && a.p.resistivity > 0.0) {
         const long sty = a.nz, stx = (long)a.ny * a.nz;
-        const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
-        const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
-        const double iz2 = 1.0 / (a.dd[2] * a.dd[2] + 1e-12);
+        const double ix2 = a.idd2[0], iy2 = a.idd2[1], iz2 = a.idd2[2];
 #pragma unroll
         for (int c = 5; c < 8; ++c) {
             const double* B = q + (size_t)c * nc + cell;
@@ -437,9 +435,7 @@ __global__ void __launch_bounds__(kThreads, 4)
         double lap[3];
         const bool resist = a.p.resistive && a.p.resistivity > 0.0;
         if (cells && mine && resist) {
-            const double ix2 = 1.0 / (a.dd[0] * a.dd[0] + 1e-12);
-            const double iy2 = 1.0 / (a.dd[1] * a.dd[1] + 1e-12);
-            const double iz2 = 1.0 / (a.dd[2] * a.dd[2] + 1e-12);
+            const double ix2 = a.idd2[0], iy2 = a.idd2[1], iz2 = a.idd2[2];
             const float* hc = halo + (warp + 3) * HZ + lane + 3;
             const float* rm = ring_at(i - 1) + warp * CZ + lane + 3;
             const float* rp = ring_at(i + 1) + warp * CZ + lane + 3;

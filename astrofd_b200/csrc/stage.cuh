@@ -42,6 +42,7 @@ struct StageArgs {
     int nv, nx, ny, nz, pitch;
     int lo, hi[3];        // updated cells [lo, hi[d]) per direction
     double dd[3], dt;
+    double idd[3], idd2[3];  // 1/dd and 1/(dd^2 + 1e-12), computed on the host
     int stage, nstages;
     long poll_limit;      // polls per tile-load wait (the default, or a test setting)
     AstroParams p;
